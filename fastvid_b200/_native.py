@@ -1,0 +1,90 @@
+"""ctypes binding of libfastvid_b200.so (include/fastvid_b200.h).
+
+The shared library is the product's compute path; there is no fallback.  If
+it is missing it is built once with nvcc (fastvid_b200/build.py); if that is
+impossible the import fails loudly.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libfastvid_b200.so"
+
+c_i32, c_i64, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p
+
+
+class Frame(ctypes.Structure):
+    """Mirror of ``fvb_frame``."""
+
+    _fields_ = [
+        ("layout", c_i32), ("bit_depth", c_i32), ("quality", c_i32), ("flags", c_i32),
+        ("width", c_i64), ("height", c_i64), ("tile_w", c_i64), ("tile_h", c_i64),
+        ("fps_num", c_i64), ("fps_den", c_i64),
+        ("tiles", c_i64), ("shards", c_i64), ("samples", c_i64),
+        ("plane_width", c_i64 * 3),
+        ("planes", c_i32), ("step", c_i32),
+        ("prefix_bytes", c_i64), ("max_stream_bytes", c_i64),
+    ]
+
+    def copy(self) -> "Frame":
+        other = Frame()
+        ctypes.memmove(ctypes.byref(other), ctypes.byref(self), ctypes.sizeof(Frame))
+        return other
+
+
+# exported symbol -> (argtypes, restype)
+SIGNATURES = {
+    "fvb_abi_version": ([], c_i32),
+    "fvb_last_error": ([], ctypes.c_char_p),
+    "fvb_encode_plan": ([c_i64, c_i64, c_i32, c_i32, c_i32, c_i64, c_i64, c_i64, c_i64,
+                         ctypes.POINTER(Frame), ctypes.POINTER(c_i64)], c_i32),
+    "fvb_encode_analyze": ([ctypes.POINTER(Frame), c_p, c_p, c_p, c_i64, c_p, ctypes.POINTER(c_i64)], c_i32),
+    "fvb_encode_emit": ([ctypes.POINTER(Frame), c_p, c_i64, c_p, c_i64, c_p], c_i32),
+    "fvb_decode_plan": ([c_p, c_i64, c_i64, ctypes.POINTER(Frame), ctypes.POINTER(c_i64)], c_i32),
+    "fvb_decode": ([ctypes.POINTER(Frame), c_p, c_i64, c_p, c_p, c_i32, c_p, c_i64, c_p], c_i32),
+    "fvb_batch_encode_plan": ([ctypes.POINTER(Frame), c_i32, ctypes.POINTER(c_i64)], c_i32),
+    "fvb_batch_encode_prepare": ([ctypes.POINTER(Frame), c_i32, c_p, c_p, c_p, c_i64, c_p], c_i32),
+    "fvb_batch_encode_enqueue": ([ctypes.POINTER(Frame), c_i32, c_p, c_i64, c_p, c_p], c_i32),
+    "fvb_batch_encode_emit": ([ctypes.POINTER(Frame), c_i32, c_p, c_i64, c_p, c_p], c_i32),
+    "fvb_batch_decode_plan": ([ctypes.POINTER(Frame), c_i32, ctypes.POINTER(c_i64)], c_i32),
+    "fvb_batch_decode_prepare": ([ctypes.POINTER(Frame), c_i32, c_p, c_p, c_p, c_p, c_p, c_i64, c_p], c_i32),
+    "fvb_batch_decode_enqueue": ([ctypes.POINTER(Frame), c_i32, c_i32, c_p, c_i64, c_p, c_p], c_i32),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load():
+    """Load (building once if absent) and return the ctypes library."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not LIB_PATH.exists():
+            from . import build as _build
+
+            _build.build()
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, (argtypes, restype) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = argtypes
+            fn.restype = restype
+        _lib = lib
+    return _lib
+
+
+def last_error() -> str:
+    msg = load().fvb_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(last_error() or f"fastvid_b200 error {rc}")

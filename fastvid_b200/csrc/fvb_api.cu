@@ -1,0 +1,638 @@
+// fvb_api.cu -- the extern "C" boundary (include/fastvid_b200.h) and the host
+// orchestration of the sm_100a kernels: argument and header validation with
+// the reference's messages, geometry, workspace layout and launch sequences.
+//
+// Host synchronisation: an encode waits once (the frame's status and stream
+// length, after every analysis pass including the device-side frame policy);
+// a decode waits once for its status word.  The reference waits after every
+// analysis pass (encode.cu:806-807) and at the end of decode (decode.cu:718).
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fastvid_b200.h"
+#include "fvb_common.cuh"
+#include "fvb_kernels.cuh"
+
+using namespace fvb;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+  g_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  g_error = std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e);
+  return FVB_ERR_CUDA;
+}
+
+#define FVB_CUDA(call)                                    \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+  } while (0)
+
+#define FVB_LAUNCHED(name)                                \
+  do {                                                    \
+    cudaError_t e_ = cudaGetLastError();                  \
+    if (e_ != cudaSuccess) return cuda_fail(e_, name);    \
+  } while (0)
+
+constexpr size_t kAlign = 256;
+size_t align_up(size_t v) { return (v + kAlign - 1) & ~(kAlign - 1); }
+
+// quality -> step (encode.cu:71-85)
+int32_t quantization_step(int64_t layout, int64_t depth, int64_t q) {
+  if ((layout == 0 && depth == 8) || (layout == 1 && depth == 8)) return 1;
+  int32_t den = 6;
+  if (layout == 1 && depth == 10) den = 20;
+  else if (layout == 1 && depth == 16) den = 24;
+  else if (layout == 2 && depth == 10) den = 10;
+  const int32_t scale = int32_t{1} << (depth - 8);
+  return 1 + static_cast<int32_t>(((100 - q) * scale + den - 1) / den);
+}
+
+int32_t refined_gray16_step(int64_t q) { return 1 + static_cast<int32_t>(((100 - q) * 256 + 7) / 8); }
+
+int64_t count_tiles(int64_t w, int64_t h, int64_t tw, int64_t th, int layout) {
+  const int planes = layout == 0 ? 1 : 3;
+  const int64_t rows = (h + th - 1) / th;
+  int64_t n = 0;
+  for (int p = 0; p < planes; ++p) {
+    const bool sub = layout == 1 && p != 0;
+    const int64_t pw = sub ? (w + 1) / 2 : w;
+    const int64_t nw = sub ? (tw + 1) / 2 : tw;
+    n += rows * ((pw + nw - 1) / nw);
+  }
+  return n;
+}
+
+int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Upper bound of one shard record: 3 header bytes plus the larger of the
+// block-pack bound and the rANS bound (table <= 1023 bytes, 28 bytes of lane
+// lengths and states, <= 12 bits per symbol plus 2 bytes per lane).
+int64_t shard_record_bound(int64_t c) {
+  const int64_t block = ceil_div(c, kBlockSymbols) + ceil_div(c * 17, 8);
+  const int64_t rans = 1023 + 28 + 4 * (ceil_div(ceil_div(c, 4) * 12, 8) + 2);
+  return 3 + (block > rans ? block : rans);
+}
+
+// Geometry of one frame into the device descriptor (tile order of
+// encode.cu:41-69; the per-row shard counts let tile_geo() find any tile's
+// first shard arithmetically).
+void build_desc(const fvb_frame& fr, FrameDesc& d, int use_med) {
+  std::memset(&d, 0, sizeof(d));
+  d.layout = fr.layout;
+  d.bit_depth = fr.bit_depth;
+  d.quality = fr.quality;
+  d.planes = fr.layout == 0 ? 1 : 3;
+  d.width = static_cast<int32_t>(fr.width);
+  d.height = static_cast<int32_t>(fr.height);
+  d.tile_w = static_cast<int32_t>(fr.tile_w);
+  d.tile_h = static_cast<int32_t>(fr.tile_h);
+  d.tiles_y = static_cast<int32_t>(ceil_div(fr.height, fr.tile_h));
+  d.last_h = static_cast<int32_t>(fr.height - static_cast<int64_t>(d.tiles_y - 1) * fr.tile_h);
+  int64_t tile = 0, shard = 0, sample = 0;
+  for (int p = 0; p < d.planes; ++p) {
+    const bool sub = fr.layout == 1 && p != 0;
+    const int64_t pw = sub ? (fr.width + 1) / 2 : fr.width;
+    const int64_t ptw = sub ? (fr.tile_w + 1) / 2 : fr.tile_w;
+    const int64_t txs = ceil_div(pw, ptw);
+    d.plane_w[p] = static_cast<int32_t>(pw);
+    d.ptile_w[p] = static_cast<int32_t>(ptw);
+    d.tiles_x[p] = static_cast<int32_t>(txs);
+    d.tile0[p] = tile;
+    d.shard0[p] = shard;
+    d.sample0[p] = sample;
+    const int64_t wl = pw - (txs - 1) * ptw;
+    for (int r = 0; r < 2; ++r) {
+      const int64_t h = r ? d.last_h : fr.tile_h;
+      d.shards_int[p][r] = static_cast<int32_t>(ceil_div(ptw * h, kShardSymbols));
+      d.shards_last[p][r] = static_cast<int32_t>(ceil_div(wl * h, kShardSymbols));
+    }
+    d.shards_row[p] = (txs - 1) * d.shards_int[p][0] + d.shards_last[p][0];
+    const int64_t plane_shards = (d.tiles_y - 1) * d.shards_row[p] + (txs - 1) * d.shards_int[p][1] + d.shards_last[p][1];
+    tile += txs * d.tiles_y;
+    shard += plane_shards;
+    sample += pw * fr.height;
+  }
+  d.tile0[d.planes] = tile;
+  d.shard0[d.planes] = shard;
+  d.sample0[d.planes] = sample;
+  d.ntiles = tile;
+  d.nshards = shard;
+  d.nsamples = sample;
+  d.max_sample = (1 << fr.bit_depth) - 1;
+  d.step0 = fr.step;
+  d.force_order0 = fr.layout == 2 && (fr.bit_depth != 10 || fr.width < 3840);
+  d.use_med0 = use_med;
+  d.prefix_bytes = kHeaderBytes + kDirBytes * tile;
+  d.fps_num = static_cast<uint32_t>(fr.fps_num);
+  d.fps_den = static_cast<uint32_t>(fr.fps_den);
+}
+
+int fill_frame(fvb_frame* fr) {
+  const int64_t tiles = count_tiles(fr->width, fr->height, fr->tile_w, fr->tile_h, fr->layout);
+  if (tiles > kMaxTiles) return fail(FVB_ERR_ARGUMENT, "too many tiles");
+  fr->planes = fr->layout == 0 ? 1 : 3;
+  const int64_t sec = fr->layout == 1 ? (fr->width + 1) / 2 : fr->width;
+  fr->plane_width[0] = fr->width;
+  fr->plane_width[1] = fr->planes == 3 ? sec : 0;
+  fr->plane_width[2] = fr->planes == 3 ? sec : 0;
+  FrameDesc d;
+  build_desc(*fr, d, 0);
+  fr->tiles = d.ntiles;
+  fr->shards = d.nshards;
+  fr->samples = d.nsamples;
+  fr->prefix_bytes = d.prefix_bytes;
+  int64_t bound = d.prefix_bytes;
+  for (int64_t t = 0; t < d.ntiles; ++t) {
+    const TileGeo g = tile_geo(d, t);
+    const int64_t s = static_cast<int64_t>(g.w) * g.h;
+    const int64_t full = s / kShardSymbols, rem = s % kShardSymbols;
+    bound += full * shard_record_bound(kShardSymbols) + (rem ? shard_record_bound(rem) : 0);
+  }
+  fr->max_stream_bytes = bound;
+  return FVB_OK;
+}
+
+int device_sms() {
+  static int sms[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!sms[dev]) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    sms[dev] = v > 0 ? v : 148;
+  }
+  return sms[dev];
+}
+
+int ensure_smem_attrs() {
+  static bool done[64] = {false};
+  int dev = 0;
+  FVB_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && done[dev]) return FVB_OK;
+  FVB_CUDA(cudaFuncSetAttribute(enc_predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(enc_predict_smem())));
+  FVB_CUDA(cudaFuncSetAttribute(enc_emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(enc_emit_smem())));
+  FVB_CUDA(cudaFuncSetAttribute(dec_reconstruct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(dec_reconstruct_smem())));
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return FVB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// workspace layouts
+
+struct Totals {
+  int64_t tiles = 0, shards = 0, samples = 0, prefix = 0;
+  bool wide = false;
+  int passes = 1;
+};
+
+Totals totals_of(const fvb_frame* frames, int n) {
+  Totals t;
+  for (int i = 0; i < n; ++i) {
+    const fvb_frame& f = frames[i];
+    t.tiles += f.tiles;
+    t.shards += f.shards;
+    t.samples += f.samples;
+    t.prefix += f.prefix_bytes;
+    const int64_t ptw0 = f.tile_w;
+    if (ptw0 > kFastMaxW) t.wide = true;
+    int passes = 1;
+    if (f.layout == 0 && f.bit_depth == 10 && f.step > 1) passes = 2;
+    if (f.layout == 0 && f.bit_depth == 16 && f.step > 1) passes = 3;
+    if (passes > t.passes) t.passes = passes;
+  }
+  return t;
+}
+
+struct EncLayout {
+  size_t frames, state, outs, queue, results, shards, folded, rans, prefix, recon, total;
+};
+
+EncLayout enc_layout(int n, const Totals& t) {
+  EncLayout w;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = o;
+    o = align_up(o + bytes);
+    return r;
+  };
+  w.frames = take(sizeof(FrameDesc) * n);
+  w.state = take(sizeof(FrameState) * n);
+  w.outs = take(sizeof(uint8_t*) * n);
+  w.queue = take(kAlign);
+  w.results = take(16 * static_cast<size_t>(n));
+  w.shards = take(sizeof(ShardInfo) * t.shards);
+  w.folded = take(4 * static_cast<size_t>(t.samples));
+  w.rans = take(static_cast<size_t>(kRansScratchBytes) * t.shards);
+  w.prefix = take(static_cast<size_t>(t.prefix));
+  w.recon = take(t.wide ? 2 * static_cast<size_t>(t.samples) : 0);
+  w.total = o;
+  return w;
+}
+
+struct DecLayout {
+  size_t frames, state, queue, results, shards, folded, total;
+};
+
+DecLayout dec_layout(int n, const Totals& t) {
+  DecLayout w;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = o;
+    o = align_up(o + bytes);
+    return r;
+  };
+  w.frames = take(sizeof(FrameDesc) * n);
+  w.state = take(sizeof(FrameState) * n);
+  w.queue = take(kAlign);
+  w.results = take(16 * static_cast<size_t>(n));
+  w.shards = take(sizeof(ShardInfo) * t.shards);
+  w.folded = take(4 * static_cast<size_t>(t.samples));
+  w.total = o;
+  return w;
+}
+
+__global__ void results_kernel(const FrameState* __restrict__ state, int n, int64_t* __restrict__ out, int decode) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[2 * i] = state[i].status;
+  out[2 * i + 1] = decode ? 0 : state[i].stream_len;
+}
+
+int check_ws(void* ws, int64_t ws_bytes, size_t need) {
+  if (!ws || ws_bytes < static_cast<int64_t>(need))
+    return fail(FVB_ERR_WORKSPACE, "workspace is smaller than planned");
+  if (reinterpret_cast<uintptr_t>(ws) & (kAlign - 1)) return fail(FVB_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+  return FVB_OK;
+}
+
+int grid_for(int64_t items, int per_cta, int ctas_per_sm) {
+  const int64_t want = ceil_div(items > 0 ? items : 1, per_cta);
+  const int64_t cap = static_cast<int64_t>(device_sms()) * ctas_per_sm;
+  return static_cast<int>(want < cap ? want : cap);
+}
+
+std::string status_message_encode(int64_t st) {
+  if (st == kStatusInternal + 1) return "tile payload is too large";
+  char buf[96];
+  std::snprintf(buf, sizeof(buf), "CUDA encoder analysis failed (status %lld)", static_cast<long long>(st));
+  return buf;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int fvb_abi_version(void) { return FVB_ABI_VERSION; }
+
+const char* fvb_last_error(void) { return g_error.c_str(); }
+
+int fvb_encode_plan(int64_t width, int64_t height, int layout, int bit_depth, int quality, int64_t fps_num,
+                    int64_t fps_den, int64_t tile_w, int64_t tile_h, fvb_frame* frame, int64_t* workspace_bytes) {
+  // argument checks in the order of encode.cu:695-716
+  if (!(layout >= 0 && layout <= 2)) return fail(FVB_ERR_ARGUMENT, "layout must be gray, yuv422, or rgb444");
+  if (!(bit_depth == 8 || bit_depth == 10 || bit_depth == 12 || bit_depth == 16))
+    return fail(FVB_ERR_ARGUMENT, "bit_depth must be 8, 10, 12, or 16");
+  if (!(quality >= 1 && quality <= 100)) return fail(FVB_ERR_ARGUMENT, "quality must be in 1..=100");
+  if (!(fps_num > 0 && fps_num <= 0xffffffffll && fps_den > 0 && fps_den <= 0xffffffffll))
+    return fail(FVB_ERR_ARGUMENT, "frame-rate components must be nonzero u32 values");
+  if (!(tile_w > 0 && tile_w <= 65535 && tile_h > 0 && tile_h <= 65535))
+    return fail(FVB_ERR_ARGUMENT, "tile dimensions must be nonzero u16 values");
+  if (!(width > 0 && height > 0 && width <= 0xffffffffll && height <= 0xffffffffll))
+    return fail(FVB_ERR_ARGUMENT, "frame dimensions must be nonzero u32 values");
+  if (width > 0x7fffffffll || height > 0x7fffffffll || width * height > (1ll << 36))
+    return fail(FVB_ERR_ARGUMENT, "frame is too large");
+  if (!frame) return fail(FVB_ERR_ARGUMENT, "frame is null");
+  std::memset(frame, 0, sizeof(*frame));
+  frame->layout = layout;
+  frame->bit_depth = bit_depth;
+  frame->quality = quality;
+  frame->width = width;
+  frame->height = height;
+  frame->tile_w = tile_w;
+  frame->tile_h = tile_h;
+  frame->fps_num = fps_num;
+  frame->fps_den = fps_den;
+  frame->step = quantization_step(layout, bit_depth, quality);
+  const int rc = fill_frame(frame);
+  if (rc) return rc;
+  if (workspace_bytes) {
+    const Totals t = totals_of(frame, 1);
+    *workspace_bytes = static_cast<int64_t>(enc_layout(1, t).total);
+  }
+  return FVB_OK;
+}
+
+int fvb_batch_encode_plan(const fvb_frame* frames, int n, int64_t* workspace_bytes) {
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  *workspace_bytes = static_cast<int64_t>(enc_layout(n, totals_of(frames, n)).total);
+  return FVB_OK;
+}
+
+int fvb_batch_encode_prepare(const fvb_frame* frames, int n, const uint16_t* const* planes, const int64_t* pitches,
+                             void* workspace, int64_t workspace_bytes, void* cuda_stream) {
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  const Totals t = totals_of(frames, n);
+  const EncLayout L = enc_layout(n, t);
+  int rc = check_ws(workspace, workspace_bytes, L.total);
+  if (rc) return rc;
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  std::vector<FrameDesc> descs(n);
+  int64_t tb = 0, sb = 0, nb = 0, pb = 0;
+  for (int i = 0; i < n; ++i) {
+    FrameDesc& d = descs[i];
+    build_desc(frames[i], d, frames[i].layout != 0);
+    for (int p = 0; p < d.planes; ++p) {
+      const uint16_t* ptr = planes[3 * i + p];
+      if (!ptr) return fail(FVB_ERR_ARGUMENT, "null plane pointer");
+      d.src[p] = ptr;
+      d.src_pitch[p] = pitches[3 * i + p];
+      if (d.src_pitch[p] < d.plane_w[p]) return fail(FVB_ERR_ARGUMENT, "plane pitch is smaller than the plane width");
+    }
+    d.tile_base = tb;
+    d.shard_base = sb;
+    d.sample_base = nb;
+    d.prefix_base = pb;
+    tb += d.ntiles;
+    sb += d.nshards;
+    nb += d.nsamples;
+    pb += d.prefix_bytes;
+  }
+  char* ws = static_cast<char*>(workspace);
+  FVB_CUDA(cudaMemcpyAsync(ws + L.frames, descs.data(), sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, stream));
+  return FVB_OK;
+}
+
+int fvb_batch_encode_enqueue(const fvb_frame* frames, int n, void* workspace, int64_t workspace_bytes,
+                             int64_t* results, void* cuda_stream) {
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  const Totals t = totals_of(frames, n);
+  const EncLayout L = enc_layout(n, t);
+  int rc = check_ws(workspace, workspace_bytes, L.total);
+  if (rc) return rc;
+  rc = ensure_smem_attrs();
+  if (rc) return rc;
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  char* ws = static_cast<char*>(workspace);
+  const FrameDesc* frames_d = reinterpret_cast<const FrameDesc*>(ws + L.frames);
+  FrameState* state = reinterpret_cast<FrameState*>(ws + L.state);
+  int* queue = reinterpret_cast<int*>(ws + L.queue);
+  ShardInfo* shards = reinterpret_cast<ShardInfo*>(ws + L.shards);
+  uint32_t* folded = reinterpret_cast<uint32_t*>(ws + L.folded);
+  uint8_t* rans = reinterpret_cast<uint8_t*>(ws + L.rans);
+  uint8_t* prefix = reinterpret_cast<uint8_t*>(ws + L.prefix);
+  uint16_t* recon = reinterpret_cast<uint16_t*>(ws + L.recon);
+  enc_init_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, n);
+  FVB_LAUNCHED("enc_init_kernel");
+  const int g_pred = grid_for(t.tiles, kWarpsPerCta, 4);
+  const int g_an = grid_for(t.shards, kWarpsPerCta, 16);
+  const int g_rans = static_cast<int>(ceil_div(t.shards * 4 > 0 ? t.shards * 4 : 1, 128));
+  for (int pass = 0; pass < t.passes; ++pass) {
+    FVB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), stream));
+    enc_predict_kernel<<<g_pred, kWarpsPerCta * 32, enc_predict_smem(), stream>>>(frames_d, state, n, t.tiles, shards,
+                                                                                 folded, queue);
+    FVB_LAUNCHED("enc_predict_kernel");
+    if (t.wide) {
+      enc_predict_wide_kernel<<<grid_for(t.tiles, 1, 8), 256, 0, stream>>>(frames_d, state, n, t.tiles, folded, recon);
+      FVB_LAUNCHED("enc_predict_wide_kernel");
+    }
+    enc_analyze_kernel<<<g_an, kWarpsPerCta * 32, 0, stream>>>(frames_d, state, n, shards, t.shards, folded, rans);
+    FVB_LAUNCHED("enc_analyze_kernel");
+    enc_rans_kernel<<<g_rans, 128, 0, stream>>>(state, shards, t.shards, folded, rans);
+    FVB_LAUNCHED("enc_rans_kernel");
+    enc_scan_kernel<<<n, 1024, 0, stream>>>(frames_d, state, n, shards, prefix);
+    FVB_LAUNCHED("enc_scan_kernel");
+  }
+  int64_t* res_d = reinterpret_cast<int64_t*>(ws + L.results);
+  results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(state, n, res_d, 0);
+  FVB_LAUNCHED("results_kernel");
+  if (results) FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
+  return FVB_OK;
+}
+
+int fvb_batch_encode_emit(const fvb_frame* frames, int n, void* workspace, int64_t workspace_bytes,
+                          uint8_t* const* outs, void* cuda_stream) {
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  const Totals t = totals_of(frames, n);
+  const EncLayout L = enc_layout(n, t);
+  int rc = check_ws(workspace, workspace_bytes, L.total);
+  if (rc) return rc;
+  rc = ensure_smem_attrs();
+  if (rc) return rc;
+  for (int i = 0; i < n; ++i)
+    if (!outs[i]) return fail(FVB_ERR_ARGUMENT, "null output pointer");
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  char* ws = static_cast<char*>(workspace);
+  uint8_t** outs_d = reinterpret_cast<uint8_t**>(ws + L.outs);
+  FVB_CUDA(cudaMemcpyAsync(outs_d, outs, sizeof(uint8_t*) * n, cudaMemcpyHostToDevice, stream));
+  const FrameDesc* frames_d = reinterpret_cast<const FrameDesc*>(ws + L.frames);
+  int64_t max_prefix = 0;
+  for (int i = 0; i < n; ++i) max_prefix = frames[i].prefix_bytes > max_prefix ? frames[i].prefix_bytes : max_prefix;
+  dim3 gp(static_cast<unsigned>(ceil_div(max_prefix, 256 * 4) > 64 ? 64 : ceil_div(max_prefix, 256 * 4)), n);
+  enc_prefix_kernel<<<gp, 256, 0, stream>>>(frames_d, n, reinterpret_cast<const uint8_t*>(ws + L.prefix), outs_d);
+  FVB_LAUNCHED("enc_prefix_kernel");
+  enc_emit_kernel<<<grid_for(t.shards, kWarpsPerCta, 8), kWarpsPerCta * 32, enc_emit_smem(), stream>>>(
+      frames_d, n, reinterpret_cast<const ShardInfo*>(ws + L.shards), t.shards,
+      reinterpret_cast<const uint32_t*>(ws + L.folded), reinterpret_cast<const uint8_t*>(ws + L.rans), outs_d);
+  FVB_LAUNCHED("enc_emit_kernel");
+  return FVB_OK;
+}
+
+int fvb_encode_analyze(const fvb_frame* frame, const uint16_t* const* planes, const int64_t* pitches, void* workspace,
+                       int64_t workspace_bytes, void* cuda_stream, int64_t* stream_len) {
+  if (!frame) return fail(FVB_ERR_ARGUMENT, "frame is null");
+  const uint16_t* p3[3] = {planes[0], frame->planes == 3 ? planes[1] : nullptr, frame->planes == 3 ? planes[2] : nullptr};
+  const int64_t q3[3] = {pitches[0], frame->planes == 3 ? pitches[1] : 0, frame->planes == 3 ? pitches[2] : 0};
+  int rc = fvb_batch_encode_prepare(frame, 1, p3, q3, workspace, workspace_bytes, cuda_stream);
+  if (rc) return rc;
+  int64_t res[2] = {0, 0};
+  rc = fvb_batch_encode_enqueue(frame, 1, workspace, workspace_bytes, res, cuda_stream);
+  if (rc) return rc;
+  FVB_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(cuda_stream)));
+  if (res[0] != 0) return fail(static_cast<int>(res[0] < kStatusInternal ? res[0] : FVB_ERR_INTERNAL),
+                               status_message_encode(res[0]));
+  if (stream_len) *stream_len = res[1];
+  return FVB_OK;
+}
+
+int fvb_encode_emit(const fvb_frame* frame, void* workspace, int64_t workspace_bytes, uint8_t* out, int64_t out_len,
+                    void* cuda_stream) {
+  if (!frame || !out) return fail(FVB_ERR_ARGUMENT, "null argument");
+  (void)out_len;
+  uint8_t* outs[1] = {out};
+  return fvb_batch_encode_emit(frame, 1, workspace, workspace_bytes, outs, cuda_stream);
+}
+
+// ---------------------------------------------------------------------------
+// decode
+
+int fvb_decode_plan(const uint8_t* b, int64_t header_len, int64_t size, fvb_frame* frame, int64_t* workspace_bytes) {
+  // fastvid_cuda.cpp:142-183, same order and messages
+  if (size < kHeaderBytes || header_len < kHeaderBytes || !b) return fail(FVB_ERR_FORMAT, "truncated Fastvid header");
+  if (std::memcmp(b, "FVID", 4) != 0) return fail(FVB_ERR_FORMAT, "bad Fastvid magic");
+  if (b[4] != 1) return fail(FVB_ERR_FORMAT, "unsupported Fastvid bitstream version");
+  if (b[5] > 2) return fail(FVB_ERR_FORMAT, "unknown pixel layout");
+  const int layout = b[5];
+  const bool gray = layout == 0;
+  const int quality = b[6];
+  if (quality < 1 || quality > 100) return fail(FVB_ERR_FORMAT, "quality is out of range");
+  const bool refined = (b[7] & 0x80) != 0;
+  const bool gray_med = (b[7] & 0x40) != 0;
+  const int depth = (b[7] & 0x3f) + 8;
+  if (!(depth == 8 || depth == 10 || depth == 12 || depth == 16)) return fail(FVB_ERR_FORMAT, "unsupported high-bit depth");
+  if (refined && !(gray && depth == 16 && quality < 100)) return fail(FVB_ERR_FORMAT, "invalid gray16 refinement flag");
+  if (gray_med && !(gray && depth == 10 && quality < 100)) return fail(FVB_ERR_FORMAT, "invalid gray MED flag");
+  auto u32 = [&](int o) {
+    return static_cast<uint32_t>(b[o]) | (static_cast<uint32_t>(b[o + 1]) << 8) | (static_cast<uint32_t>(b[o + 2]) << 16) |
+           (static_cast<uint32_t>(b[o + 3]) << 24);
+  };
+  const int64_t width = u32(8), height = u32(12);
+  const int64_t tw = b[16] | (b[17] << 8), th = b[18] | (b[19] << 8);
+  if (!(width > 0 && height > 0 && tw > 0 && th > 0)) return fail(FVB_ERR_FORMAT, "zero dimension");
+  if (u32(20) == 0 || u32(24) == 0) return fail(FVB_ERR_FORMAT, "zero frame-rate component");
+  const int64_t tile_count = u32(28);
+  const int64_t expected = count_tiles(width, height, tw, th, layout);
+  if (tile_count != expected) return fail(FVB_ERR_FORMAT, "tile count does not match dimensions");
+  if (tile_count > kMaxTiles) return fail(FVB_ERR_FORMAT, "too many tiles");
+  if (kHeaderBytes + tile_count * kDirBytes > size) return fail(FVB_ERR_FORMAT, "truncated tile directory");
+  if (width > 0x7fffffffll || height > 0x7fffffffll || width * height > (1ll << 36))
+    return fail(FVB_ERR_FORMAT, "frame is too large");
+  if (!frame) return fail(FVB_ERR_ARGUMENT, "frame is null");
+  std::memset(frame, 0, sizeof(*frame));
+  frame->layout = layout;
+  frame->bit_depth = depth;
+  frame->quality = quality;
+  frame->flags = b[7] & 0xc0;
+  frame->width = width;
+  frame->height = height;
+  frame->tile_w = tw;
+  frame->tile_h = th;
+  frame->fps_num = u32(20);
+  frame->fps_den = u32(24);
+  frame->step = refined ? refined_gray16_step(quality) : quantization_step(layout, depth, quality);
+  int rc = fill_frame(frame);
+  if (rc) return rc;
+  if (workspace_bytes) *workspace_bytes = static_cast<int64_t>(dec_layout(1, totals_of(frame, 1)).total);
+  return FVB_OK;
+}
+
+int fvb_batch_decode_plan(const fvb_frame* frames, int n, int64_t* workspace_bytes) {
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  *workspace_bytes = static_cast<int64_t>(dec_layout(n, totals_of(frames, n)).total);
+  return FVB_OK;
+}
+
+int fvb_batch_decode_prepare(const fvb_frame* frames, int n, const uint8_t* const* streams, const int64_t* stream_lens,
+                             uint16_t* const* planes, const int64_t* pitches, void* workspace, int64_t workspace_bytes,
+                             void* cuda_stream) {
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  const Totals t = totals_of(frames, n);
+  const DecLayout L = dec_layout(n, t);
+  int rc = check_ws(workspace, workspace_bytes, L.total);
+  if (rc) return rc;
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  std::vector<FrameDesc> descs(n);
+  int64_t tb = 0, sb = 0, nb = 0;
+  for (int i = 0; i < n; ++i) {
+    FrameDesc& d = descs[i];
+    const bool gray = frames[i].layout == 0;
+    build_desc(frames[i], d, ((frames[i].flags & 0x40) != 0) || !gray);
+    if (!streams[i]) return fail(FVB_ERR_ARGUMENT, "null stream pointer");
+    d.stream = streams[i];
+    d.stream_len = stream_lens[i];
+    for (int p = 0; p < d.planes; ++p) {
+      if (!planes[3 * i + p]) return fail(FVB_ERR_ARGUMENT, "null plane pointer");
+      d.dst[p] = planes[3 * i + p];
+      d.dst_pitch[p] = pitches[3 * i + p];
+      if (d.dst_pitch[p] < d.plane_w[p]) return fail(FVB_ERR_ARGUMENT, "plane pitch is smaller than the plane width");
+    }
+    d.tile_base = tb;
+    d.shard_base = sb;
+    d.sample_base = nb;
+    tb += d.ntiles;
+    sb += d.nshards;
+    nb += d.nsamples;
+  }
+  char* ws = static_cast<char*>(workspace);
+  FVB_CUDA(cudaMemcpyAsync(ws + L.frames, descs.data(), sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, stream));
+  return FVB_OK;
+}
+
+int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void* workspace, int64_t workspace_bytes,
+                             int64_t* results, void* cuda_stream) {
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  const Totals t = totals_of(frames, n);
+  const DecLayout L = dec_layout(n, t);
+  int rc = check_ws(workspace, workspace_bytes, L.total);
+  if (rc) return rc;
+  rc = ensure_smem_attrs();
+  if (rc) return rc;
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  char* ws = static_cast<char*>(workspace);
+  const FrameDesc* frames_d = reinterpret_cast<const FrameDesc*>(ws + L.frames);
+  FrameState* state = reinterpret_cast<FrameState*>(ws + L.state);
+  int* queue = reinterpret_cast<int*>(ws + L.queue);
+  ShardInfo* shards = reinterpret_cast<ShardInfo*>(ws + L.shards);
+  uint32_t* folded = reinterpret_cast<uint32_t*>(ws + L.folded);
+  FVB_CUDA(cudaMemsetAsync(state, 0, sizeof(FrameState) * n, stream));
+  FVB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), stream));
+  dec_parse_kernel<<<grid_for(t.tiles, 128, 8), 128, 0, stream>>>(frames_d, state, n, t.tiles, shards);
+  FVB_LAUNCHED("dec_parse_kernel");
+  dec_shards_kernel<<<grid_for(t.shards, kWarpsPerCta, 16), kWarpsPerCta * 32, 0, stream>>>(frames_d, state, shards,
+                                                                                            t.shards, folded);
+  FVB_LAUNCHED("dec_shards_kernel");
+  if (wavefront) {
+    dec_reconstruct_kernel<<<grid_for(t.tiles, kWarpsPerCta, 4), kWarpsPerCta * 32, dec_reconstruct_smem(), stream>>>(
+        frames_d, state, n, t.tiles, folded, queue);
+    FVB_LAUNCHED("dec_reconstruct_kernel");
+    if (t.wide) {
+      dec_reconstruct_wide_kernel<<<grid_for(t.tiles, 1, 8), 256, 0, stream>>>(frames_d, state, n, t.tiles, folded);
+      FVB_LAUNCHED("dec_reconstruct_wide_kernel");
+    }
+  } else {
+    dec_reconstruct_serial_kernel<<<static_cast<int>(ceil_div(t.tiles, 128)), 128, 0, stream>>>(frames_d, state, n,
+                                                                                               t.tiles, folded);
+    FVB_LAUNCHED("dec_reconstruct_serial_kernel");
+  }
+  int64_t* res_d = reinterpret_cast<int64_t*>(ws + L.results);
+  results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(state, n, res_d, 1);
+  FVB_LAUNCHED("results_kernel");
+  if (results) FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
+  return FVB_OK;
+}
+
+int fvb_decode(const fvb_frame* frame, const uint8_t* stream, int64_t stream_len, uint16_t* const* planes,
+               const int64_t* pitches, int wavefront, void* workspace, int64_t workspace_bytes, void* cuda_stream) {
+  if (!frame) return fail(FVB_ERR_ARGUMENT, "frame is null");
+  uint16_t* p3[3] = {planes[0], frame->planes == 3 ? planes[1] : nullptr, frame->planes == 3 ? planes[2] : nullptr};
+  const int64_t q3[3] = {pitches[0], frame->planes == 3 ? pitches[1] : 0, frame->planes == 3 ? pitches[2] : 0};
+  const uint8_t* s1[1] = {stream};
+  const int64_t l1[1] = {stream_len};
+  int rc = fvb_batch_decode_prepare(frame, 1, s1, l1, p3, q3, workspace, workspace_bytes, cuda_stream);
+  if (rc) return rc;
+  int64_t res[2] = {0, 0};
+  rc = fvb_batch_decode_enqueue(frame, 1, wavefront, workspace, workspace_bytes, res, cuda_stream);
+  if (rc) return rc;
+  FVB_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(cuda_stream)));
+  if (res[0] != 0) {
+    char buf[96];
+    std::snprintf(buf, sizeof(buf), "malformed entropy payload (CUDA status %lld)", static_cast<long long>(res[0]));
+    return fail(static_cast<int>(res[0]), buf);
+  }
+  return FVB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,48 @@
+// fvb_kernels.cuh -- launch shapes and kernel declarations shared by the
+// kernel files and the host orchestration (fvb_api.cu).
+#pragma once
+
+#include "fvb_common.cuh"
+
+namespace fvb {
+
+constexpr int kWarpsPerCta = 4;    // warps per CTA of the warp-per-item kernels
+constexpr int kSrcStride = 68;     // u16 ring row stride (64 columns + skew pad)
+constexpr int kFoldStride = 66;    // u32 ring row stride (64 columns + skew pad)
+constexpr int kFastMaxW = 512;     // widest tile of the register-wavefront path
+
+// encoder
+__global__ void enc_init_kernel(const FrameDesc* frames, FrameState* state, int nframes);
+__global__ void enc_predict_kernel(const FrameDesc* frames, FrameState* state, int nframes,
+                                   int64_t total_tiles, ShardInfo* shards, uint32_t* folded, int* queue);
+__global__ void enc_predict_wide_kernel(const FrameDesc* frames, FrameState* state, int nframes,
+                                        int64_t total_tiles, uint32_t* folded, uint16_t* recon);
+__global__ void enc_analyze_kernel(const FrameDesc* frames, FrameState* state, int nframes, ShardInfo* shards,
+                                   int64_t total_shards, const uint32_t* folded, uint8_t* rans_scratch);
+__global__ void enc_rans_kernel(const FrameState* state, ShardInfo* shards, int64_t total_shards,
+                                const uint32_t* folded, uint8_t* rans_scratch);
+__global__ void enc_scan_kernel(const FrameDesc* frames, FrameState* state, int nframes, ShardInfo* shards,
+                                uint8_t* prefix);
+__global__ void enc_emit_kernel(const FrameDesc* frames, int nframes, const ShardInfo* shards,
+                                int64_t total_shards, const uint32_t* folded, const uint8_t* rans_scratch,
+                                uint8_t* const* outs);
+__global__ void enc_prefix_kernel(const FrameDesc* frames, int nframes, const uint8_t* prefix,
+                                  uint8_t* const* outs);
+
+// decoder
+__global__ void dec_parse_kernel(const FrameDesc* frames, FrameState* state, int nframes, int64_t total_tiles,
+                                 ShardInfo* shards);
+__global__ void dec_shards_kernel(const FrameDesc* frames, FrameState* state, const ShardInfo* shards,
+                                  int64_t total_shards, uint32_t* folded);
+__global__ void dec_reconstruct_kernel(const FrameDesc* frames, const FrameState* state, int nframes,
+                                       int64_t total_tiles, const uint32_t* folded, int* queue);
+__global__ void dec_reconstruct_wide_kernel(const FrameDesc* frames, const FrameState* state, int nframes,
+                                            int64_t total_tiles, const uint32_t* folded);
+__global__ void dec_reconstruct_serial_kernel(const FrameDesc* frames, const FrameState* state, int nframes,
+                                              int64_t total_tiles, const uint32_t* folded);
+
+size_t enc_predict_smem();
+size_t enc_emit_smem();
+size_t dec_reconstruct_smem();
+
+}  // namespace fvb

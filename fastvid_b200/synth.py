@@ -1,0 +1,207 @@
+"""Seeded synthetic frames standing in for the reference's image corpus.
+
+The reference measures on a corpus of photographs that is not available
+here.  These frames follow the workload descriptions instead: a sum of four
+low-frequency sinusoid layers (periods 32-256 px, random orientation and
+phase), axis-aligned constant rectangles with sharp edges, and near-Gaussian
+noise, clipped to the bit depth and stored as uint16 planes.
+
+Everything is integer arithmetic (a Bhaskara-I sine table, a counter-based
+32-bit hash for noise, Irwin-Hall sums for the Gaussian shape), so the same
+seed gives the same samples on every machine and numpy build.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+_TABLE_BITS = 10
+_TABLE = None
+
+
+def _sine_table() -> np.ndarray:
+    """1024-entry sine in [-32767, 32767] from Bhaskara I's rational formula."""
+    global _TABLE
+    if _TABLE is None:
+        half = 1 << (_TABLE_BITS - 1)
+        u = np.arange(half, dtype=np.int64)
+        num = 16 * u * (half - u) * 32767
+        den = 5 * half * half - 4 * u * (half - u)
+        s = num // den
+        _TABLE = np.concatenate([s, -s]).astype(np.int64)
+    return _TABLE
+
+
+def _hash32(x: np.ndarray) -> np.ndarray:
+    """lowbias32 integer hash (C. Wellons) on uint32."""
+    x = x.astype(np.uint32, copy=True)
+    x ^= x >> np.uint32(16)
+    x *= np.uint32(0x7FEB352D)
+    x ^= x >> np.uint32(15)
+    x *= np.uint32(0x846CA68B)
+    x ^= x >> np.uint32(16)
+    return x
+
+
+def _noise(count: int, seed: int, sigma_num: int, sigma_den: int) -> np.ndarray:
+    """Near-Gaussian integer noise with standard deviation sigma_num/sigma_den.
+
+    Sum of four 12-bit uniforms (Irwin-Hall, sd 4096/sqrt(3)); scaled by
+    sigma*sqrt(3)/4096 with sqrt(3) ~ 1732/1000, rounded to nearest.
+    """
+    if sigma_num == 0:
+        return np.zeros(count, dtype=np.int64)
+    idx = np.arange(count, dtype=np.uint64)
+    key = np.uint32((seed * 0x9E3779B1) & 0xFFFFFFFF)
+    acc = np.zeros(count, dtype=np.int64)
+    for j in range(2):
+        h = _hash32((idx * np.uint64(2) + np.uint64(j)).astype(np.uint32) ^ key)
+        acc += (h & np.uint32(0xFFF)).astype(np.int64) + ((h >> np.uint32(16)) & np.uint32(0xFFF)).astype(np.int64)
+    centred = acc * 2 - 4 * 4095                      # 2x, mean zero
+    scale_num = sigma_num * 1732
+    scale_den = sigma_den * 1000 * 4096 * 2
+    return (centred * scale_num * 2 + scale_den) // (2 * scale_den)
+
+
+@dataclass(frozen=True)
+class PlaneSpec:
+    mean: int
+    amplitude: int
+    rects: int
+    sigma_num: int
+    sigma_den: int = 1
+
+
+def _field(width: int, height: int, rng: np.random.Generator, amplitude: int) -> np.ndarray:
+    """Zero-mean sum of 4 sinusoid layers with amplitudes summing to `amplitude`."""
+    table = _sine_table()
+    y = np.arange(height, dtype=np.int64)[:, None]
+    x = np.arange(width, dtype=np.int64)[None, :]
+    weights = rng.integers(1, 100, size=4)
+    amps = (weights * amplitude) // weights.sum()
+    out = np.zeros((height, width), dtype=np.int64)
+    for a in amps:
+        # spatial frequency |k| in [1024, 8192] table units / 256 px -> periods 32..256 px
+        while True:
+            kx, ky = (int(v) for v in rng.integers(-8192, 8193, size=2))
+            n2 = kx * kx + ky * ky
+            if 1024 * 1024 <= n2 <= 8192 * 8192:
+                break
+        phase = int(rng.integers(0, 1 << _TABLE_BITS))
+        arg = ((x * kx + y * ky) >> 8) + phase
+        out += (table[arg & ((1 << _TABLE_BITS) - 1)] * int(a)) >> 15
+    return out
+
+
+def _rectangles(plane: np.ndarray, rng: np.random.Generator, count: int, maximum: int) -> None:
+    h, w = plane.shape
+    for _ in range(count):
+        rw = int(rng.integers(max(1, w // 16), max(2, w // 4)))
+        rh = int(rng.integers(max(1, h // 16), max(2, h // 4)))
+        x0 = int(rng.integers(0, max(1, w - rw)))
+        y0 = int(rng.integers(0, max(1, h - rh)))
+        plane[y0:y0 + rh, x0:x0 + rw] = int(rng.integers(0, maximum + 1))
+
+
+def make_frame(width: int, height: int, layout: str, bit_depth: int, seed: int, *,
+               amplitude: int | None = None, mean: int | None = None, rects: int = 10,
+               sigma: tuple[int, int] = (2, 1), correlation: bool = True):
+    """One frame as a tuple of (H, W) uint16 numpy planes.
+
+    `sigma` is a rational (numerator, denominator).  For rgb444 the sinusoid
+    fields are correlated across planes (0.8 shared + 0.6 independent).
+    """
+    maximum = (1 << bit_depth) - 1
+    if mean is None:
+        mean = (maximum + 1) // 2
+    if amplitude is None:
+        amplitude = (60 * (maximum + 1)) // 256
+    rng = np.random.default_rng(seed)
+    plane_count = 1 if layout == "gray" else 3
+    widths = [width] + [((width + 1) // 2) if layout == "yuv422" else width] * (plane_count - 1)
+    shared = _field(width, height, rng, amplitude) if (layout == "rgb444" and correlation) else None
+    planes = []
+    for p in range(plane_count):
+        pw = widths[p]
+        field = _field(pw, height, rng, amplitude)
+        if shared is not None:
+            field = (4 * shared + 3 * field) // 5
+        plane = field + mean
+        _rectangles(plane, rng, rects, maximum)
+        plane = plane + _noise(pw * height, seed * 7 + p + 1, *sigma).reshape(height, pw)
+        planes.append(np.clip(plane, 0, maximum).astype(np.uint16))
+    return tuple(planes)
+
+
+# Workloads of the benchmark configurations (sizes, formats, coding params).
+CONFIGS = {
+    "gray8_512": dict(width=512, height=512, layout="gray", bit_depth=8, quality=100, tile=(64, 64),
+                      gen=dict(seed=1, rects=10, sigma=(2, 1))),
+    "rgb8_1080p": dict(width=1920, height=1080, layout="rgb444", bit_depth=8, quality=90, tile=(64, 64),
+                       gen=dict(seed=2, rects=10, sigma=(3, 1))),
+    "gray16_4k": dict(width=3840, height=2160, layout="gray", bit_depth=16, quality=87, tile=(128, 128),
+                      gen=dict(seed=5, rects=20, sigma=(40, 1), amplitude=20000, mean=32768)),
+    "rgb10_4k": dict(width=3840, height=2160, layout="rgb444", bit_depth=10, quality=85, tile=(128, 128),
+                     gen=dict(seed=6, rects=10, sigma=(4, 1))),
+}
+
+
+def config_frame(name: str):
+    c = CONFIGS[name]
+    return make_frame(c["width"], c["height"], c["layout"], c["bit_depth"], **c["gen"])
+
+
+def mixed_batch_specs(frames: int = 96):
+    """The 96-frame uneven mix: 32x 720p gray8, 32x 1080p RGB8, 16x 4K RGB10,
+    16x 2048x1080 gray16, per-frame seeds 1000+i, every 4th frame near-flat
+    (noise sd 0.5).  Scaled proportionally for other frame counts."""
+    groups = [
+        (frames // 3, dict(width=1280, height=720, layout="gray", bit_depth=8, quality=100)),
+        (frames // 3, dict(width=1920, height=1080, layout="rgb444", bit_depth=8, quality=90)),
+        (frames // 6, dict(width=3840, height=2160, layout="rgb444", bit_depth=10, quality=85)),
+        (frames - 2 * (frames // 3) - frames // 6,
+         dict(width=2048, height=1080, layout="gray", bit_depth=16, quality=87)),
+    ]
+    specs = []
+    i = 0
+    for count, base in groups:
+        for _ in range(count):
+            flat = i % 4 == 3
+            spec = dict(base)
+            spec["seed"] = 1000 + i
+            spec["sigma"] = (1, 2) if flat else ((40, 1) if base["bit_depth"] == 16 else (3, 1))
+            spec["amplitude"] = (20000 if base["bit_depth"] == 16 else None)
+            spec["mean"] = (32768 if base["bit_depth"] == 16 else None)
+            spec["rects"] = 20 if base["bit_depth"] == 16 else 10
+            specs.append(spec)
+            i += 1
+    return specs
+
+
+def frame_from_spec(spec):
+    return make_frame(spec["width"], spec["height"], spec["layout"], spec["bit_depth"], spec["seed"],
+                      amplitude=spec.get("amplitude"), mean=spec.get("mean"), rects=spec.get("rects", 10),
+                      sigma=spec.get("sigma", (2, 1)))
+
+
+def reference_pattern(layout: str, width: int, height: int, bit_depth: int, pattern: str = "polynomial"):
+    """The deterministic planes of the reference test suite (cuda/tests/test_codec.py:9-30)."""
+    maximum = (1 << bit_depth) - 1
+    widths = [width] if layout == "gray" else [
+        width,
+        (width + 1) // 2 if layout == "yuv422" else width,
+        (width + 1) // 2 if layout == "yuv422" else width,
+    ]
+    planes = []
+    for seed, pw in enumerate(widths, 1):
+        i = np.arange(pw * height, dtype=np.int64)
+        if pattern == "zero":
+            v = np.zeros_like(i)
+        elif pattern == "ramp":
+            v = i * (seed * 2 + 1) + seed * 17
+        else:
+            v = i * (977 + seed * 13) + i * i * 17 + seed * 131
+        planes.append((v % (maximum + 1)).astype(np.uint16).reshape(height, pw))
+    return tuple(planes)

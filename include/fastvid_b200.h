@@ -1,0 +1,142 @@
+/*
+ * fastvid_b200.h -- C ABI of the B200 (sm_100a) fastvid intra codec.
+ *
+ * Plain C types only: device pointers, sizes, an opaque CUDA stream handle
+ * (a cudaStream_t passed as void*), and int status codes.  The caller owns
+ * every buffer (workspace, inputs, outputs); the library allocates no device
+ * memory.  Streams are byte-identical to the reference encoder
+ * (generative-workflows/fastvid cuda/csrc/encode.cu) and decodes are bit-exact.
+ *
+ * Status codes: 0 is success.  Positive codes are the reference's device
+ * status codes, unchanged: encoder 1 = a sample above 2^bit_depth-1,
+ * 2 = a shard body above 65535 bytes; decoder 1 zero-run, 2 Rice, 3 block pack,
+ * 4 unknown mode, 5 rANS, 10 tile directory, 11 shard header.  Negative codes
+ * are host-side rejections (below).  fvb_last_error() returns the message of
+ * the calling thread's last failure; the messages of argument and header
+ * checks are the reference's own (cuda/csrc/encode.cu:695-735,
+ * cuda/csrc/fastvid_cuda.cpp:142-183).
+ */
+#ifndef FASTVID_B200_H
+#define FASTVID_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FVB_ABI_VERSION 1
+
+enum {
+  FVB_OK = 0,
+  FVB_ERR_ARGUMENT = -1,  /* invalid argument */
+  FVB_ERR_FORMAT = -2,    /* stream header rejected on the host */
+  FVB_ERR_WORKSPACE = -3, /* workspace or output smaller than required */
+  FVB_ERR_CUDA = -4,      /* CUDA runtime failure */
+  FVB_ERR_INTERNAL = -5   /* consistency check of this library failed */
+};
+
+/* One frame's parameters and derived geometry.  Filled by fvb_encode_plan or
+ * fvb_decode_plan; the caller treats it as read-only. */
+typedef struct fvb_frame {
+  int32_t layout;     /* 0 gray, 1 yuv422, 2 rgb444 */
+  int32_t bit_depth;  /* 8, 10, 12, 16 */
+  int32_t quality;    /* 1..100 */
+  int32_t flags;      /* decode: header byte 7 high bits (0x40 gray MED, 0x80 refined gray16) */
+  int64_t width, height, tile_w, tile_h;
+  int64_t fps_num, fps_den;
+  int64_t tiles, shards, samples; /* geometry (reference encode.cu:41-69) */
+  int64_t plane_width[3];
+  int32_t planes;
+  int32_t step;       /* quantizer step before the frame policy (encode) / of the stream (decode) */
+  int64_t prefix_bytes;     /* 32 + 32 * tiles */
+  int64_t max_stream_bytes; /* upper bound of the encoded size */
+} fvb_frame;
+
+int fvb_abi_version(void);
+const char* fvb_last_error(void);
+
+/* ---- single frame (the drop-in path) -------------------------------------
+ *
+ * Encode = fvb_encode_plan + fvb_encode_analyze + fvb_encode_emit, which
+ * together replace fastvid_encode_cuda (reference cuda/csrc/encode.cu:686-931,
+ * bound as _C.encode at cuda/csrc/fastvid_cuda.cpp:366-377).
+ */
+
+/* Validates the arguments exactly as encode.cu:695-716 does and computes the
+ * geometry and the workspace size (bytes, device memory). */
+int fvb_encode_plan(int64_t width, int64_t height, int layout, int bit_depth, int quality,
+                    int64_t fps_num, int64_t fps_den, int64_t tile_w, int64_t tile_h,
+                    fvb_frame* frame, int64_t* workspace_bytes);
+
+/* Predicts, analyses and lays out the stream on `cuda_stream` (the frame
+ * policy of encode.cu:812-847 runs on the device), then waits for the one
+ * 96-byte result read and returns the exact stream length.  planes[p] are
+ * device pointers to uint16 planes with row pitch pitches[p] (elements).
+ * Replaces encode.cu:727-870. */
+int fvb_encode_analyze(const fvb_frame* frame, const uint16_t* const* planes, const int64_t* pitches,
+                       void* workspace, int64_t workspace_bytes, void* cuda_stream, int64_t* stream_len);
+
+/* Writes the stream (header, directory, shard records) into device buffer
+ * `out` of out_len >= stream_len bytes; asynchronous on `cuda_stream`.
+ * Replaces encode.cu:871-931. */
+int fvb_encode_emit(const fvb_frame* frame, void* workspace, int64_t workspace_bytes, uint8_t* out,
+                    int64_t out_len, void* cuda_stream);
+
+/* Validates the 32-byte header (host memory) against the stream length,
+ * exactly as fastvid_cuda.cpp:142-183, and computes geometry and workspace.
+ * Replaces the host half of the binding's decode (fastvid_cuda.cpp:141-236). */
+int fvb_decode_plan(const uint8_t* header, int64_t header_len, int64_t stream_len, fvb_frame* frame,
+                    int64_t* workspace_bytes);
+
+/* Decodes a device-resident stream into device planes (planes[p] with row
+ * pitch pitches[p] elements), wavefront (1) or serial (0) reconstruction;
+ * waits for the status word.  Replaces fastvid_decode_cuda
+ * (cuda/csrc/decode.cu:660-730) including the device metadata parse. */
+int fvb_decode(const fvb_frame* frame, const uint8_t* stream, int64_t stream_len, uint16_t* const* planes,
+               const int64_t* pitches, int wavefront, void* workspace, int64_t workspace_bytes,
+               void* cuda_stream);
+
+/* ---- batches (no reference counterpart: the reference batches with a Python
+ * loop over the single-frame path, fastvid/__init__.py:44-53,63) ------------
+ *
+ * All frames share one launch of each kernel; per-frame bytes are identical
+ * to the single-frame path. */
+
+int fvb_batch_encode_plan(const fvb_frame* frames, int n, int64_t* workspace_bytes);
+
+/* Uploads the frame table (planes: 3 pointers per frame, pitches likewise). */
+int fvb_batch_encode_prepare(const fvb_frame* frames, int n, const uint16_t* const* planes,
+                             const int64_t* pitches, void* workspace, int64_t workspace_bytes,
+                             void* cuda_stream);
+
+/* Enqueues every analysis pass; no host synchronisation, so it can be
+ * captured into a CUDA graph.  Copies n result records (status, stream
+ * length) into `results` (pinned host memory, 2 int64 per frame). */
+int fvb_batch_encode_enqueue(const fvb_frame* frames, int n, void* workspace, int64_t workspace_bytes,
+                             int64_t* results, void* cuda_stream);
+
+/* After the results are visible: writes frame i's stream at outs[i]
+ * (host array of device pointers, one per frame; uploaded from pageable
+ * memory, so this call is not capturable).  Asynchronous. */
+int fvb_batch_encode_emit(const fvb_frame* frames, int n, void* workspace, int64_t workspace_bytes,
+                          uint8_t* const* outs, void* cuda_stream);
+
+int fvb_batch_decode_plan(const fvb_frame* frames, int n, int64_t* workspace_bytes);
+
+/* streams[i]/stream_lens[i]: device streams; planes: 3 device pointers per
+ * frame, pitches likewise.  Uploads the frame table. */
+int fvb_batch_decode_prepare(const fvb_frame* frames, int n, const uint8_t* const* streams,
+                             const int64_t* stream_lens, uint16_t* const* planes, const int64_t* pitches,
+                             void* workspace, int64_t workspace_bytes, void* cuda_stream);
+
+/* Enqueues parse, entropy decode and reconstruction for every frame (graph
+ * capturable) and copies one int64 status per frame into `results`. */
+int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void* workspace,
+                             int64_t workspace_bytes, int64_t* results, void* cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTVID_B200_H */
