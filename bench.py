@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""Benchmark of the fastvid intra codec on B200: batched encode+decode of the
+96-frame uneven mix, Gpix/s (luma pixels of all frames / step time).
+
+One step = encode every frame of the batch and decode every stream again,
+inputs resident in HBM (1.3 GB, above the 126 MB L2, so no flush is needed).
+Prints one JSON line (rank 0).  ``--impl reference`` times the CPU restatement
+of the reference codec (the reference has no CPU codec of its own) on all host
+cores over a bounded sample of the same workload.
+
+Launch: python bench.py [--gpus N] [--steps K] [--warmup W]
+        python -m torch.distributed.run --nproc-per-node N ... bench.py --gpus N
+With N > 1 every rank runs its own replica of the batch (weak scaling, no
+collective on the data path); times are the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import signal
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = ("mixed96: 32x 1280x720 gray8 q100 tile64, 32x 1920x1080 rgb444-8 q90 tile64, "
+            "16x 3840x2160 rgb444-10 q85 tile128, 16x 2048x1080 gray16 q87 tile128; "
+            "every 4th frame near-flat (noise sd 0.5)")
+TILES = {("gray", 8): (64, 64), ("rgb444", 8): (64, 64), ("rgb444", 10): (128, 128), ("gray", 16): (128, 128)}
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    p.add_argument("--frames", type=int, default=96)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
+    return p.parse_args()
+
+
+def _gen(spec):
+    from fastvid_b200 import synth
+
+    return synth.frame_from_spec(spec)
+
+
+def generate(specs, workers):
+    import multiprocessing as mp
+
+    if workers <= 1:
+        return [_gen(s) for s in specs]
+    with mp.get_context("spawn").Pool(workers) as pool:
+        return pool.map(_gen, specs, chunksize=1)
+
+
+def cpu_sample(specs):
+    """One frame of each format: the bounded CPU sample."""
+    seen, out = set(), []
+    for i, s in enumerate(specs):
+        key = (s["layout"], s["bit_depth"])
+        if key not in seen:
+            seen.add(key)
+            out.append(i)
+    return out
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.send_signal(signal.SIGTERM)
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except OSError:
+            pass
+        finally:
+            if self.path:
+                try:
+                    os.unlink(self.path)
+                except OSError:
+                    pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in rows for j in range(4) if r[5 + j] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def time_oracle(frames, specs, idx, budget_s):
+    """Encode+decode the sample frames with the oracle on all host cores."""
+    import oracle
+
+    threads = oracle.cpu_threads()
+    pixels = sum(specs[i]["width"] * specs[i]["height"] for i in idx)
+    reps, total = 0, 0.0
+    t_start = time.perf_counter()
+    while True:
+        t0 = time.perf_counter()
+        for i in idx:
+            s = specs[i]
+            stream = oracle.encode(frames[i], layout=s["layout"], bit_depth=s["bit_depth"], quality=s["quality"],
+                                   tile_size=TILES[(s["layout"], s["bit_depth"])], threads=threads)
+            oracle.decode(stream, threads=threads)
+        total += time.perf_counter() - t0
+        reps += 1
+        if time.perf_counter() - t_start >= budget_s or reps >= 50:
+            break
+    return pixels * reps / total / 1e9, threads, reps
+
+
+def run_reference(args, specs):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    idx = cpu_sample(specs)
+    frames = {i: _gen(specs[i]) for i in idx}
+    fl = [frames.get(i) for i in range(len(specs))]
+    for _ in range(max(1, args.warmup)):
+        time_oracle(fl, specs, idx, 0.0)
+    t0 = time.perf_counter()
+    values = []
+    for _ in range(args.steps):
+        g, threads, reps = time_oracle(fl, specs, idx, 0.0)
+        values.append(g)
+    elapsed = time.perf_counter() - t0
+    value = statistics.median(values)
+    sample = f"frames {idx} (one per format) encode+decode per step, {threads} threads"
+    line = {
+        "impl": "reference", "metric": "Gpix/s encode+decode", "value": value, "unit": "Gpix/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "frames": len(specs), "parallelism": "replicas"},
+        "cpu_baseline": {"value": value, "unit": "Gpix/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# Algorithmic bytes per sample of each stage (encode: 2 B in + stream out;
+# decode: stream in + 2 B out).  A kernel is charged its stage's figure.
+ENC_KERNELS = {"enc_init", "enc_predict", "enc_predict_wide", "enc_analyze", "enc_rans", "enc_scan", "enc_prefix",
+               "enc_emit"}
+
+
+def main():
+    args = parse_args()
+    from fastvid_b200 import synth
+
+    specs = synth.mixed_batch_specs(args.frames)
+    for s in specs:
+        s["tile"] = TILES[(s["layout"], s["bit_depth"])]
+    if args.impl == "reference":
+        return run_reference(args, specs)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    workers = max(1, min(16, (os.cpu_count() or 2) // max(1, world)))
+    host_frames = generate(specs, workers)
+
+    import numpy as np
+    import torch
+
+    import fastvid_b200
+    from fastvid_b200 import _native
+    from fastvid_b200.batch import BatchCodec
+
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=device)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # inputs resident in HBM, plus pinned host copies for the end-to-end leg
+    pinned = [tuple(torch.from_numpy(np.ascontiguousarray(p)).pin_memory() for p in f) for f in host_frames]
+    dev_frames = [tuple(p.to(device, non_blocking=True) for p in f) for f in pinned]
+    torch.cuda.synchronize()
+    layouts = [s["layout"] for s in specs]
+    depths = [s["bit_depth"] for s in specs]
+    quals = [s["quality"] for s in specs]
+    tiles = [s["tile"] for s in specs]
+    luma = sum(s["width"] * s["height"] for s in specs)
+    samples = sum(p.size for f in host_frames for p in f)
+    codec = BatchCodec(device, use_graphs=False)
+
+    def step(frames_dev):
+        streams = codec.encode(frames_dev, layout=layouts, bit_depth=depths, quality=quals, tile_size=tiles)
+        planes = codec.decode(streams)
+        return streams, planes
+
+    for _ in range(max(1, args.warmup)):
+        streams, planes = step(dev_frames)
+    torch.cuda.synchronize()
+
+    # bit-exactness: lossless frames round trip exactly; every frame's bytes
+    # equal the single-frame path's; decodes equal the single-frame decode
+    bit_exact = True
+    for i, (s, f) in enumerate(zip(specs, dev_frames)):
+        if s["quality"] == 100 or (s["bit_depth"] == 8 and s["layout"] == "gray"):
+            bit_exact &= all(torch.equal(a, b) for a, b in zip(planes[i], f))
+    for i in cpu_sample(specs):
+        plain = fastvid_b200.encode(dev_frames[i], layout=layouts[i], bit_depth=depths[i], quality=quals[i],
+                                    tile_size=tiles[i])
+        bit_exact &= torch.equal(plain, streams[i])
+        bit_exact &= all(torch.equal(a, b) for a, b in zip(fastvid_b200.decode(plain), planes[i]))
+    stream_bytes = sum(int(s.numel()) for s in streams)
+
+    # timed region
+    barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = _native.launch_count()
+    with Clocks(local_rank) as clocks, _native.KernelProfile() as prof:
+        for k in range(args.steps):
+            a, b, c = ev[k]
+            a.record()
+            streams = codec.encode(dev_frames, layout=layouts, bit_depth=depths, quality=quals, tile_size=tiles)
+            b.record()
+            planes = codec.decode(streams)
+            c.record()
+        torch.cuda.synchronize()
+    barrier()
+    launches = _native.launch_count() - launches0
+    enc_ms = sum(a.elapsed_time(b) for a, b, _ in ev) / args.steps
+    dec_ms = sum(b.elapsed_time(c) for _, b, c in ev) / args.steps
+    step_ms = max_over_ranks(enc_ms + dec_ms)
+    enc_ms = max_over_ranks(enc_ms)
+    dec_ms = max_over_ranks(dec_ms)
+    value = world * luma / (step_ms / 1e3) / 1e9
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_kind = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    kernel_ms = {k: v / args.steps for k, v in prof.ms.items()}
+    kernel_launches = {k: v // args.steps for k, v in prof.launches.items()}
+    dominant = max(kernel_ms, key=kernel_ms.get)
+    enc_bytes = 2 * samples + stream_bytes
+    dec_bytes = stream_bytes + 2 * samples
+    stage_bytes = enc_bytes if dominant in ENC_KERNELS else dec_bytes
+    per_launch_ms = kernel_ms[dominant] / max(1, kernel_launches[dominant])
+    per_launch_bytes = stage_bytes / max(1, kernel_launches[dominant])
+    achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        rec = tr.get(dominant)
+        if rec:
+            traffic = rec["bytes_per_sample"] * samples / max(1, kernel_launches[dominant])
+    except (OSError, ValueError, KeyError):
+        pass
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": per_launch_bytes, "launch_ms": per_launch_ms}
+    pipeline = (enc_bytes + dec_bytes) / (step_ms / 1e3) / 1e9
+    line = {
+        "metric": "Gpix/s encode+decode", "value": value, "unit": "Gpix/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16",
+        "data": "synthetic (seeded integer generator standing in for the unavailable corpus)",
+        "config": {"workload": WORKLOAD, "frames": len(specs), "luma_pixels": luma, "samples": samples,
+                   "form": "batched (one launch per kernel for the whole batch)",
+                   "l2": "inputs 1.3 GB > 126 MB L2 (no flush needed)", "parallelism": f"replicas x{world}"},
+        "enc_gpix_s": world * luma / (enc_ms / 1e3) / 1e9, "dec_gpix_s": world * luma / (dec_ms / 1e3) / 1e9,
+        "enc_ms": enc_ms, "dec_ms": dec_ms, "stream_bytes": stream_bytes, "bit_exact": bool(bit_exact),
+        "roofline": roofline,
+        "pipeline_roofline": {"achieved": pipeline, "peak": hbm_peak, "unit": "GB/s", "frac": pipeline / hbm_peak,
+                              "bytes_per_step": enc_bytes + dec_bytes},
+        "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(kernel_ms.items(), key=lambda kv: -kv[1])},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+
+    # single-frame (plain, drop-in) path on the same frames, for the batched/plain ratio
+    if not args.no_plain:
+        def plain_step():
+            out = []
+            for i, f in enumerate(dev_frames):
+                st = fastvid_b200.encode(f, layout=layouts[i], bit_depth=depths[i], quality=quals[i],
+                                         tile_size=tiles[i])
+                out.append(fastvid_b200.decode(st))
+            return out
+
+        plain_step()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        plain_step()
+        b.record()
+        b.synchronize()
+        plain_ms = max_over_ranks(a.elapsed_time(b))
+        line["plain_gpix_s"] = world * luma / (plain_ms / 1e3) / 1e9
+        line["batched_over_plain"] = line["value"] / line["plain_gpix_s"]
+
+    # end to end through the public API with host buffers
+    if not args.no_e2e:
+        out_planes = [tuple(torch.empty(p.shape, dtype=torch.uint16).pin_memory() for p in f) for f in pinned]
+        host_streams = None
+
+        def e2e_step():
+            nonlocal host_streams
+            frames_d = [tuple(p.to(device, non_blocking=True) for p in f) for f in pinned]
+            st = codec.encode(frames_d, layout=layouts, bit_depth=depths, quality=quals, tile_size=tiles)
+            host_streams = [torch.empty(s.numel(), dtype=torch.uint8).pin_memory() if host_streams is None
+                            else host_streams[i] for i, s in enumerate(st)]
+            for hs, s in zip(host_streams, st):
+                hs.copy_(s, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            dst = [hs.to(device, non_blocking=True) for hs in host_streams]
+            dec = codec.decode(dst)
+            for op, dp in zip(out_planes, dec):
+                for o, d in zip(op, dp):
+                    o.copy_(d, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+
+        e2e_step()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        k_e2e = max(1, min(args.steps, 3))
+        for _ in range(k_e2e):
+            e2e_step()
+        b.record()
+        b.synchronize()
+        e2e_ms = max_over_ranks(a.elapsed_time(b) / k_e2e)
+        frame_bytes = 2 * samples
+        line["e2e"] = {"value": world * luma / (e2e_ms / 1e3) / 1e9, "unit": "Gpix/s",
+                       "h2d_bytes_per_step": frame_bytes + stream_bytes,
+                       "d2h_bytes_per_step": stream_bytes + frame_bytes, "ms_per_step": e2e_ms,
+                       "path": "pinned host frames -> encode -> host streams -> decode -> pinned host planes"}
+        roundtrip_ok = all(np.array_equal(o.numpy(), h) for op, hf, s in zip(out_planes, host_frames, specs)
+                           if s["quality"] == 100 for o, h in zip(op, hf))
+        line["bit_exact"] = bool(line["bit_exact"] and roundtrip_ok)
+
+    # CPU baseline: the oracle (restatement of the reference) on all host cores
+    if rank == 0 and world == 1 and not args.no_cpu:
+        idx = cpu_sample(specs)
+        gpix, threads, reps = time_oracle(host_frames, specs, idx, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": gpix, "unit": "Gpix/s", "cores": threads, "kind": "port",
+                                "sample": f"frames {idx} (one per format), encode+decode, {reps} reps"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -40,6 +40,11 @@ class Frame(ctypes.Structure):
 SIGNATURES = {
     "fvb_abi_version": ([], c_i32),
     "fvb_last_error": ([], ctypes.c_char_p),
+    "fvb_launch_count": ([], c_i64),
+    "fvb_kernel_count": ([], c_i32),
+    "fvb_kernel_name": ([c_i32], ctypes.c_char_p),
+    "fvb_profile_begin": ([], c_i32),
+    "fvb_profile_end": ([c_p, c_p, c_i32], c_i32),
     "fvb_encode_plan": ([c_i64, c_i64, c_i32, c_i32, c_i32, c_i64, c_i64, c_i64, c_i64,
                          ctypes.POINTER(Frame), ctypes.POINTER(c_i64)], c_i32),
     "fvb_encode_analyze": ([ctypes.POINTER(Frame), c_p, c_p, c_p, c_i64, c_p, ctypes.POINTER(c_i64)], c_i32),
@@ -83,6 +88,38 @@ def load():
 def last_error() -> str:
     msg = load().fvb_last_error()
     return msg.decode() if msg else ""
+
+
+def kernel_names() -> list[str]:
+    lib = load()
+    return [lib.fvb_kernel_name(i).decode() for i in range(lib.fvb_kernel_count())]
+
+
+class KernelProfile:
+    """Context manager: per-kernel device time (ms) and launch counts of the
+    library's launches issued by this thread inside the block."""
+
+    def __enter__(self):
+        check(load().fvb_profile_begin())
+        self.ms = {}
+        self.launches = {}
+        return self
+
+    def __exit__(self, *exc):
+        lib = load()
+        n = lib.fvb_kernel_count()
+        ms = (ctypes.c_double * n)()
+        cnt = (c_i64 * n)()
+        check(lib.fvb_profile_end(ms, cnt, n))
+        for i, name in enumerate(kernel_names()):
+            if cnt[i]:
+                self.ms[name] = ms[i]
+                self.launches[name] = cnt[i]
+        return False
+
+
+def launch_count() -> int:
+    return int(load().fvb_launch_count())
 
 
 def check(rc: int) -> None:

@@ -18,6 +18,7 @@ from . import _native
 from ._native import Frame
 
 _U32_MAX = 0xFFFFFFFF
+_LAYOUTS_DEFAULT = {"gray": 0, "yuv422": 1, "rgb444": 2}
 
 
 def _fail(msg: str):
@@ -125,7 +126,7 @@ def header_of(encoded: torch.Tensor) -> bytes:
     return bytes(head.contiguous().numpy().tobytes())
 
 
-def plan_decode(encoded: torch.Tensor):
+def plan_decode(encoded: torch.Tensor, header: bytes | None = None):
     """Validate like fastvid_cuda.cpp:142-183; returns (frame, workspace_bytes)."""
     if encoded.dtype != torch.uint8:
         _fail("encoded must have dtype uint8")
@@ -136,7 +137,8 @@ def plan_decode(encoded: torch.Tensor):
     size = encoded.numel()
     if size < 32:
         _fail("truncated Fastvid header")
-    header = header_of(encoded)
+    if header is None:
+        header = header_of(encoded)
     lib = _native.load()
     frame = Frame()
     ws = ctypes.c_int64()

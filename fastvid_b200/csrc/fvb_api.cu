@@ -6,6 +6,7 @@
 // length, after every analysis pass including the device-side frame policy);
 // a decode waits once for its status word.  The reference waits after every
 // analysis pass (encode.cu:806-807) and at the end of decode (decode.cu:718).
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -42,6 +43,64 @@ int cuda_fail(cudaError_t e, const char* where) {
     cudaError_t e_ = cudaGetLastError();                  \
     if (e_ != cudaSuccess) return cuda_fail(e_, name);    \
   } while (0)
+
+// ---------------------------------------------------------------------------
+// Launch accounting and optional per-kernel timing.  Every kernel launch of
+// this library is counted; while profiling is on, each launch is bracketed
+// by CUDA events on its own stream and the elapsed times are summed per
+// kernel when profiling ends.
+enum KernelId {
+  K_ENC_INIT, K_ENC_PREDICT, K_ENC_PREDICT_WIDE, K_ENC_ANALYZE, K_ENC_RANS, K_ENC_SCAN, K_ENC_PREFIX,
+  K_ENC_EMIT, K_DEC_PARSE, K_DEC_SHARDS, K_DEC_RECON, K_DEC_RECON_WIDE, K_DEC_RECON_SERIAL, K_RESULTS,
+  K_COUNT
+};
+const char* const kKernelNames[K_COUNT] = {
+    "enc_init", "enc_predict", "enc_predict_wide", "enc_analyze", "enc_rans", "enc_scan", "enc_prefix",
+    "enc_emit", "dec_parse", "dec_shards", "dec_reconstruct", "dec_reconstruct_wide",
+    "dec_reconstruct_serial", "results"};
+
+std::atomic<int64_t> g_launches{0};
+
+struct ProfRecord {
+  int kernel;
+  cudaEvent_t a, b;
+};
+struct Profiler {
+  bool on = false;
+  std::vector<ProfRecord> records;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t get() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+};
+thread_local Profiler g_prof;
+
+struct LaunchScope {
+  int kernel;
+  cudaStream_t stream;
+  cudaEvent_t a = nullptr;
+  LaunchScope(int k, cudaStream_t s) : kernel(k), stream(s) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (g_prof.on) {
+      a = g_prof.get();
+      cudaEventRecord(a, stream);
+    }
+  }
+  ~LaunchScope() {
+    if (a) {
+      cudaEvent_t b = g_prof.get();
+      cudaEventRecord(b, stream);
+      g_prof.records.push_back({kernel, a, b});
+    }
+  }
+};
 
 constexpr size_t kAlign = 256;
 size_t align_up(size_t v) { return (v + kAlign - 1) & ~(kAlign - 1); }
@@ -275,6 +334,15 @@ int check_ws(void* ws, int64_t ws_bytes, size_t need) {
   if (!ws || ws_bytes < static_cast<int64_t>(need))
     return fail(FVB_ERR_WORKSPACE, "workspace is smaller than planned");
   if (reinterpret_cast<uintptr_t>(ws) & (kAlign - 1)) return fail(FVB_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+  // launch on the device that owns the workspace
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, ws) == cudaSuccess && attr.type == cudaMemoryTypeDevice) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != attr.device) FVB_CUDA(cudaSetDevice(attr.device));
+  } else {
+    cudaGetLastError();
+    return fail(FVB_ERR_WORKSPACE, "workspace must be device memory");
+  }
   return FVB_OK;
 }
 
@@ -297,6 +365,43 @@ std::string status_message_encode(int64_t st) {
 extern "C" {
 
 int fvb_abi_version(void) { return FVB_ABI_VERSION; }
+
+int64_t fvb_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int fvb_kernel_count(void) { return K_COUNT; }
+
+const char* fvb_kernel_name(int kernel) { return kernel >= 0 && kernel < K_COUNT ? kKernelNames[kernel] : ""; }
+
+int fvb_profile_begin(void) {
+  for (auto& r : g_prof.records) {
+    g_prof.pool.push_back(r.a);
+    g_prof.pool.push_back(r.b);
+  }
+  g_prof.records.clear();
+  g_prof.on = true;
+  return FVB_OK;
+}
+
+int fvb_profile_end(double* ms, int64_t* launches, int n) {
+  g_prof.on = false;
+  for (int i = 0; i < n; ++i) {
+    if (ms) ms[i] = 0.0;
+    if (launches) launches[i] = 0;
+  }
+  for (auto& r : g_prof.records) {
+    FVB_CUDA(cudaEventSynchronize(r.b));
+    float t = 0.f;
+    FVB_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+    if (r.kernel < n) {
+      if (ms) ms[r.kernel] += t;
+      if (launches) launches[r.kernel] += 1;
+    }
+    g_prof.pool.push_back(r.a);
+    g_prof.pool.push_back(r.b);
+  }
+  g_prof.records.clear();
+  return FVB_OK;
+}
 
 const char* fvb_last_error(void) { return g_error.c_str(); }
 
@@ -395,29 +500,50 @@ int fvb_batch_encode_enqueue(const fvb_frame* frames, int n, void* workspace, in
   uint8_t* rans = reinterpret_cast<uint8_t*>(ws + L.rans);
   uint8_t* prefix = reinterpret_cast<uint8_t*>(ws + L.prefix);
   uint16_t* recon = reinterpret_cast<uint16_t*>(ws + L.recon);
-  enc_init_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, n);
+  {
+    LaunchScope scope_(K_ENC_INIT, stream);
+    enc_init_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, n);
+  }
   FVB_LAUNCHED("enc_init_kernel");
   const int g_pred = grid_for(t.tiles, kWarpsPerCta, 4);
   const int g_an = grid_for(t.shards, kWarpsPerCta, 16);
   const int g_rans = static_cast<int>(ceil_div(t.shards * 4 > 0 ? t.shards * 4 : 1, 128));
   for (int pass = 0; pass < t.passes; ++pass) {
     FVB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), stream));
-    enc_predict_kernel<<<g_pred, kWarpsPerCta * 32, enc_predict_smem(), stream>>>(frames_d, state, n, t.tiles, shards,
-                                                                                 folded, queue);
+    {
+      LaunchScope scope_(K_ENC_PREDICT, stream);
+      enc_predict_kernel<<<g_pred, kWarpsPerCta * 32, enc_predict_smem(), stream>>>(frames_d, state, n, t.tiles, shards,
+                                                                                   folded, queue);
+    }
     FVB_LAUNCHED("enc_predict_kernel");
     if (t.wide) {
-      enc_predict_wide_kernel<<<grid_for(t.tiles, 1, 8), 256, 0, stream>>>(frames_d, state, n, t.tiles, folded, recon);
+      {
+        LaunchScope scope_(K_ENC_PREDICT_WIDE, stream);
+        enc_predict_wide_kernel<<<grid_for(t.tiles, 1, 8), 256, 0, stream>>>(frames_d, state, n, t.tiles, folded, recon);
+      }
       FVB_LAUNCHED("enc_predict_wide_kernel");
     }
-    enc_analyze_kernel<<<g_an, kWarpsPerCta * 32, 0, stream>>>(frames_d, state, n, shards, t.shards, folded, rans);
+    {
+      LaunchScope scope_(K_ENC_ANALYZE, stream);
+      enc_analyze_kernel<<<g_an, kWarpsPerCta * 32, 0, stream>>>(frames_d, state, n, shards, t.shards, folded, rans);
+    }
     FVB_LAUNCHED("enc_analyze_kernel");
-    enc_rans_kernel<<<g_rans, 128, 0, stream>>>(state, shards, t.shards, folded, rans);
+    {
+      LaunchScope scope_(K_ENC_RANS, stream);
+      enc_rans_kernel<<<g_rans, 128, 0, stream>>>(state, shards, t.shards, folded, rans);
+    }
     FVB_LAUNCHED("enc_rans_kernel");
-    enc_scan_kernel<<<n, 1024, 0, stream>>>(frames_d, state, n, shards, prefix);
+    {
+      LaunchScope scope_(K_ENC_SCAN, stream);
+      enc_scan_kernel<<<n, 1024, 0, stream>>>(frames_d, state, n, shards, prefix);
+    }
     FVB_LAUNCHED("enc_scan_kernel");
   }
   int64_t* res_d = reinterpret_cast<int64_t*>(ws + L.results);
-  results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(state, n, res_d, 0);
+  {
+    LaunchScope scope_(K_RESULTS, stream);
+    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(state, n, res_d, 0);
+  }
   FVB_LAUNCHED("results_kernel");
   if (results) FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
   return FVB_OK;
@@ -442,11 +568,17 @@ int fvb_batch_encode_emit(const fvb_frame* frames, int n, void* workspace, int64
   int64_t max_prefix = 0;
   for (int i = 0; i < n; ++i) max_prefix = frames[i].prefix_bytes > max_prefix ? frames[i].prefix_bytes : max_prefix;
   dim3 gp(static_cast<unsigned>(ceil_div(max_prefix, 256 * 4) > 64 ? 64 : ceil_div(max_prefix, 256 * 4)), n);
-  enc_prefix_kernel<<<gp, 256, 0, stream>>>(frames_d, n, reinterpret_cast<const uint8_t*>(ws + L.prefix), outs_d);
+  {
+    LaunchScope scope_(K_ENC_PREFIX, stream);
+    enc_prefix_kernel<<<gp, 256, 0, stream>>>(frames_d, n, reinterpret_cast<const uint8_t*>(ws + L.prefix), outs_d);
+  }
   FVB_LAUNCHED("enc_prefix_kernel");
-  enc_emit_kernel<<<grid_for(t.shards, kWarpsPerCta, 8), kWarpsPerCta * 32, enc_emit_smem(), stream>>>(
-      frames_d, n, reinterpret_cast<const ShardInfo*>(ws + L.shards), t.shards,
-      reinterpret_cast<const uint32_t*>(ws + L.folded), reinterpret_cast<const uint8_t*>(ws + L.rans), outs_d);
+  {
+    LaunchScope scope_(K_ENC_EMIT, stream);
+    enc_emit_kernel<<<grid_for(t.shards, kWarpsPerCta, 8), kWarpsPerCta * 32, enc_emit_smem(), stream>>>(
+        frames_d, n, reinterpret_cast<const ShardInfo*>(ws + L.shards), t.shards,
+        reinterpret_cast<const uint32_t*>(ws + L.folded), reinterpret_cast<const uint8_t*>(ws + L.rans), outs_d);
+  }
   FVB_LAUNCHED("enc_emit_kernel");
   return FVB_OK;
 }
@@ -589,26 +721,44 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
   uint32_t* folded = reinterpret_cast<uint32_t*>(ws + L.folded);
   FVB_CUDA(cudaMemsetAsync(state, 0, sizeof(FrameState) * n, stream));
   FVB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), stream));
-  dec_parse_kernel<<<grid_for(t.tiles, 128, 8), 128, 0, stream>>>(frames_d, state, n, t.tiles, shards);
+  {
+    LaunchScope scope_(K_DEC_PARSE, stream);
+    dec_parse_kernel<<<grid_for(t.tiles, 128, 8), 128, 0, stream>>>(frames_d, state, n, t.tiles, shards);
+  }
   FVB_LAUNCHED("dec_parse_kernel");
-  dec_shards_kernel<<<grid_for(t.shards, kWarpsPerCta, 16), kWarpsPerCta * 32, 0, stream>>>(frames_d, state, shards,
-                                                                                            t.shards, folded);
+  {
+    LaunchScope scope_(K_DEC_SHARDS, stream);
+    dec_shards_kernel<<<grid_for(t.shards, kWarpsPerCta, 16), kWarpsPerCta * 32, 0, stream>>>(frames_d, state, shards,
+                                                                                              t.shards, folded);
+  }
   FVB_LAUNCHED("dec_shards_kernel");
   if (wavefront) {
-    dec_reconstruct_kernel<<<grid_for(t.tiles, kWarpsPerCta, 4), kWarpsPerCta * 32, dec_reconstruct_smem(), stream>>>(
-        frames_d, state, n, t.tiles, folded, queue);
+    {
+      LaunchScope scope_(K_DEC_RECON, stream);
+      dec_reconstruct_kernel<<<grid_for(t.tiles, kWarpsPerCta, 4), kWarpsPerCta * 32, dec_reconstruct_smem(), stream>>>(
+          frames_d, state, n, t.tiles, folded, queue);
+    }
     FVB_LAUNCHED("dec_reconstruct_kernel");
     if (t.wide) {
-      dec_reconstruct_wide_kernel<<<grid_for(t.tiles, 1, 8), 256, 0, stream>>>(frames_d, state, n, t.tiles, folded);
+      {
+        LaunchScope scope_(K_DEC_RECON_WIDE, stream);
+        dec_reconstruct_wide_kernel<<<grid_for(t.tiles, 1, 8), 256, 0, stream>>>(frames_d, state, n, t.tiles, folded);
+      }
       FVB_LAUNCHED("dec_reconstruct_wide_kernel");
     }
   } else {
-    dec_reconstruct_serial_kernel<<<static_cast<int>(ceil_div(t.tiles, 128)), 128, 0, stream>>>(frames_d, state, n,
-                                                                                               t.tiles, folded);
+    {
+      LaunchScope scope_(K_DEC_RECON_SERIAL, stream);
+      dec_reconstruct_serial_kernel<<<static_cast<int>(ceil_div(t.tiles, 128)), 128, 0, stream>>>(frames_d, state, n,
+                                                                                                 t.tiles, folded);
+    }
     FVB_LAUNCHED("dec_reconstruct_serial_kernel");
   }
   int64_t* res_d = reinterpret_cast<int64_t*>(ws + L.results);
-  results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(state, n, res_d, 1);
+  {
+    LaunchScope scope_(K_RESULTS, stream);
+    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(state, n, res_d, 1);
+  }
   FVB_LAUNCHED("results_kernel");
   if (results) FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
   return FVB_OK;

@@ -56,6 +56,20 @@ typedef struct fvb_frame {
 int fvb_abi_version(void);
 const char* fvb_last_error(void);
 
+/* ---- instrumentation (no reference counterpart; the reference profiles
+ * with torch.profiler around whole calls, cuda/benchmarks/profile_*.py) ---- */
+
+/* Number of kernel launches this library has issued in the process. */
+int64_t fvb_launch_count(void);
+/* Kernel identifiers 0..fvb_kernel_count()-1 and their names. */
+int fvb_kernel_count(void);
+const char* fvb_kernel_name(int kernel);
+/* While profiling is on (per calling thread), every launch is bracketed by
+ * CUDA events on its stream; fvb_profile_end waits for them and writes, per
+ * kernel id, the summed milliseconds and the number of launches. */
+int fvb_profile_begin(void);
+int fvb_profile_end(double* ms, int64_t* launches, int n);
+
 /* ---- single frame (the drop-in path) -------------------------------------
  *
  * Encode = fvb_encode_plan + fvb_encode_analyze + fvb_encode_emit, which
