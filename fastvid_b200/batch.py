@@ -70,6 +70,9 @@ class BatchCodec:
         self.max_cached = max_cached_shapes
         self._enc: dict = {}
         self._dec: dict = {}
+        self._plans: dict = {}
+        self._dec_plans: dict = {}
+        self._hdr_scratch = None
         self.lib = _native.load()
 
     # ---- encode -----------------------------------------------------------
@@ -117,13 +120,22 @@ class BatchCodec:
                 lay = 0 if len(planes) == 1 else (1 if planes[1].shape[1] != planes[0].shape[1] else 2)
             elif isinstance(lay, str):
                 lay = _LAYOUTS_DEFAULT[lay]
-            frame, _, views, pit = plan_encode(list(planes), lay, depths[i], qualities[i], rates[i][0], rates[i][1],
-                                               tiles[i][0], tiles[i][1])
-            if views[0].device != self.device:
-                raise RuntimeError("all frames of a batch must be on the codec's device")
+            key = (lay, depths[i], qualities[i], tuple(rates[i]), tuple(tiles[i]),
+                   tuple((p.shape, p.dtype, p.device, p.stride()) for p in planes))
+            hit = self._plans.get(key)
+            if hit is not None:
+                frame, pit = hit
+                views = planes
+            else:
+                frame, _, views, pit = plan_encode(list(planes), lay, depths[i], qualities[i], rates[i][0],
+                                                   rates[i][1], tiles[i][0], tiles[i][1])
+                if views[0].device != self.device:
+                    raise RuntimeError("all frames of a batch must be on the codec's device")
+                if all(v is p for v, p in zip(views, planes)):  # no copy was needed: cacheable
+                    self._plans[key] = (frame, pit)
             plans.append(frame)
             ptrs.extend([v.data_ptr() for v in views] + [0] * (3 - len(views)))
-            pitches.extend(pit + [0] * (3 - len(pit)))
+            pitches.extend(list(pit) + [0] * (3 - len(pit)))
         with torch.cuda.device(self.device):
             slot = self._encode_slot(plans)
             cur = torch.cuda.current_stream(self.device)
@@ -209,10 +221,25 @@ class BatchCodec:
             s = s.contiguous()
             dev_streams.append(s if s.device == self.device else s.to(self.device))
         with torch.cuda.device(self.device):
-            heads = torch.stack([s[:32] for s in dev_streams]).cpu()
+            cur = torch.cuda.current_stream(self.device)
+            need = ((16 * n + 255) // 256) * 256 + 32 * n
+            if self._hdr_scratch is None or self._hdr_scratch.numel() < need:
+                self._hdr_scratch = torch.empty(max(need, 1 << 16), dtype=torch.uint8, device=self.device)
+            heads = ctypes.create_string_buffer(32 * n)
+            s_arr = (ctypes.c_void_p * n)(*[s.data_ptr() for s in dev_streams])
+            l_arr = (ctypes.c_int64 * n)(*[s.numel() for s in dev_streams])
+            _native.check(self.lib.fvb_gather_headers(s_arr, l_arr, n, self._hdr_scratch.data_ptr(),
+                                                      self._hdr_scratch.numel(), heads, cur.cuda_stream))
+            raw = heads.raw
             plans = []
-            for s, h in zip(dev_streams, heads):
-                plans.append(plan_decode(s, header=bytes(h.numpy().tobytes()))[0])
+            for i, s in enumerate(dev_streams):
+                header = raw[32 * i:32 * i + 32]
+                key = (header, s.numel())
+                frame = self._dec_plans.get(key)
+                if frame is None:
+                    frame = plan_decode(s, header=header)[0]
+                    self._dec_plans[key] = frame
+                plans.append(frame)
             slot = self._decode_slot(plans, predictor == "wavefront")
             total = sum(f.samples for f in plans)
             arena = torch.empty(total, dtype=torch.uint16, device=self.device)
@@ -223,9 +250,6 @@ class BatchCodec:
                 out_planes.append(tuple(pv))
                 ptrs.extend([p.data_ptr() for p in pv] + [0] * (3 - len(pv)))
                 pitches.extend([p.size(1) for p in pv] + [0] * (3 - len(pv)))
-            cur = torch.cuda.current_stream(self.device)
-            s_arr = (ctypes.c_void_p * n)(*[s.data_ptr() for s in dev_streams])
-            l_arr = (ctypes.c_int64 * n)(*[s.numel() for s in dev_streams])
             p_arr = (ctypes.c_void_p * (3 * n))(*ptrs)
             q_arr = (ctypes.c_int64 * (3 * n))(*pitches)
             _native.check(self.lib.fvb_batch_decode_prepare(slot.frames, n, s_arr, l_arr, p_arr, q_arr,

@@ -52,12 +52,13 @@ int cuda_fail(cudaError_t e, const char* where) {
 enum KernelId {
   K_ENC_INIT, K_ENC_PREDICT, K_ENC_PREDICT_WIDE, K_ENC_ANALYZE, K_ENC_RANS, K_ENC_SCAN, K_ENC_PREFIX,
   K_ENC_EMIT, K_DEC_PARSE, K_DEC_SHARDS, K_DEC_RECON, K_DEC_RECON_WIDE, K_DEC_RECON_SERIAL, K_RESULTS,
-  K_COUNT
+  K_DEC_RANS, K_DEC_OTHER, K_COUNT
 };
 const char* const kKernelNames[K_COUNT] = {
     "enc_init", "enc_predict", "enc_predict_wide", "enc_analyze", "enc_rans", "enc_scan", "enc_prefix",
-    "enc_emit", "dec_parse", "dec_shards", "dec_reconstruct", "dec_reconstruct_wide",
-    "dec_reconstruct_serial", "results"};
+    "enc_emit", "dec_parse", "dec_rans_tables", "dec_reconstruct", "dec_reconstruct_wide",
+    "dec_reconstruct_serial", "results", "dec_rans", "dec_other"};
+constexpr int kGroupShards = 8;
 
 std::atomic<int64_t> g_launches{0};
 
@@ -244,6 +245,8 @@ int ensure_smem_attrs() {
                                 static_cast<int>(enc_emit_smem())));
   FVB_CUDA(cudaFuncSetAttribute(dec_reconstruct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(dec_reconstruct_smem())));
+  FVB_CUDA(cudaFuncSetAttribute(dec_rans_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(dec_rans_smem())));
   if (dev >= 0 && dev < 64) done[dev] = true;
   return FVB_OK;
 }
@@ -302,7 +305,7 @@ EncLayout enc_layout(int n, const Totals& t) {
 }
 
 struct DecLayout {
-  size_t frames, state, queue, results, shards, folded, total;
+  size_t frames, state, queue, results, shards, lists, items, tables, folded, total;
 };
 
 DecLayout dec_layout(int n, const Totals& t) {
@@ -318,9 +321,20 @@ DecLayout dec_layout(int n, const Totals& t) {
   w.queue = take(kAlign);
   w.results = take(16 * static_cast<size_t>(n));
   w.shards = take(sizeof(ShardInfo) * t.shards);
+  w.lists = take(sizeof(DecodeLists));
+  w.items = take(4 * 4 * static_cast<size_t>(t.shards));
+  w.tables = take(dec_rans_table_bytes() * static_cast<size_t>(t.shards));
   w.folded = take(4 * static_cast<size_t>(t.samples));
   w.total = o;
   return w;
+}
+
+__global__ void gather_headers_kernel(const uint8_t* const* __restrict__ streams, const int64_t* __restrict__ lens,
+                                      int n, uint8_t* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * kHeaderBytes) return;
+  const int k = i / kHeaderBytes, b = i % kHeaderBytes;
+  out[i] = b < lens[k] ? streams[k][b] : 0;
 }
 
 __global__ void results_kernel(const FrameState* __restrict__ state, int n, int64_t* __restrict__ out, int decode) {
@@ -661,6 +675,33 @@ int fvb_decode_plan(const uint8_t* b, int64_t header_len, int64_t size, fvb_fram
   return FVB_OK;
 }
 
+int fvb_gather_headers(const uint8_t* const* streams, const int64_t* stream_lens, int n, void* scratch,
+                       int64_t scratch_bytes, uint8_t* headers, void* cuda_stream) {
+  if (n <= 0 || !streams || !headers) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  const size_t need = align_up(16 * static_cast<size_t>(n)) + kHeaderBytes * static_cast<size_t>(n);
+  int rc = check_ws(scratch, scratch_bytes, need);
+  if (rc) return rc;
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  char* ws = static_cast<char*>(scratch);
+  std::vector<uint64_t> table(2 * static_cast<size_t>(n));
+  for (int i = 0; i < n; ++i) {
+    table[i] = reinterpret_cast<uint64_t>(streams[i]);
+    table[n + i] = static_cast<uint64_t>(stream_lens[i]);
+  }
+  FVB_CUDA(cudaMemcpyAsync(ws, table.data(), 16 * static_cast<size_t>(n), cudaMemcpyHostToDevice, stream));
+  uint8_t* out_d = reinterpret_cast<uint8_t*>(ws + align_up(16 * static_cast<size_t>(n)));
+  {
+    LaunchScope scope_(K_RESULTS, stream);
+    gather_headers_kernel<<<static_cast<int>(ceil_div(n * kHeaderBytes, 256)), 256, 0, stream>>>(
+        reinterpret_cast<const uint8_t* const*>(ws), reinterpret_cast<const int64_t*>(ws + 8 * static_cast<size_t>(n)),
+        n, out_d);
+  }
+  FVB_LAUNCHED("gather_headers_kernel");
+  FVB_CUDA(cudaMemcpyAsync(headers, out_d, kHeaderBytes * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
+  FVB_CUDA(cudaStreamSynchronize(stream));
+  return FVB_OK;
+}
+
 int fvb_batch_decode_plan(const fvb_frame* frames, int n, int64_t* workspace_bytes) {
   if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
   *workspace_bytes = static_cast<int64_t>(dec_layout(n, totals_of(frames, n)).total);
@@ -719,19 +760,36 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
   int* queue = reinterpret_cast<int*>(ws + L.queue);
   ShardInfo* shards = reinterpret_cast<ShardInfo*>(ws + L.shards);
   uint32_t* folded = reinterpret_cast<uint32_t*>(ws + L.folded);
+  DecodeLists* lists = reinterpret_cast<DecodeLists*>(ws + L.lists);
+  int32_t* items = reinterpret_cast<int32_t*>(ws + L.items);
   FVB_CUDA(cudaMemsetAsync(state, 0, sizeof(FrameState) * n, stream));
   FVB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), stream));
+  FVB_CUDA(cudaMemsetAsync(lists, 0, sizeof(DecodeLists), stream));
   {
     LaunchScope scope_(K_DEC_PARSE, stream);
-    dec_parse_kernel<<<grid_for(t.tiles, 128, 8), 128, 0, stream>>>(frames_d, state, n, t.tiles, shards);
+    dec_parse_kernel<<<grid_for(t.tiles, 128, 8), 128, 0, stream>>>(frames_d, state, n, t.tiles, shards, t.shards,
+                                                                       lists, items);
   }
   FVB_LAUNCHED("dec_parse_kernel");
+  RansTable* tables = reinterpret_cast<RansTable*>(ws + L.tables);
   {
     LaunchScope scope_(K_DEC_SHARDS, stream);
-    dec_shards_kernel<<<grid_for(t.shards, kWarpsPerCta, 16), kWarpsPerCta * 32, 0, stream>>>(frames_d, state, shards,
-                                                                                              t.shards, folded);
+    dec_rans_tables_kernel<<<grid_for(t.shards, 128, 16), 128, 0, stream>>>(frames_d, state, shards, lists, items,
+                                                                           tables);
   }
-  FVB_LAUNCHED("dec_shards_kernel");
+  FVB_LAUNCHED("dec_rans_tables_kernel");
+  {
+    LaunchScope scope_(K_DEC_RANS, stream);
+    dec_rans_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), 1, 12), 32, dec_rans_smem(), stream>>>(
+        frames_d, state, shards, lists, items, tables, folded);
+  }
+  FVB_LAUNCHED("dec_rans_kernel");
+  {
+    LaunchScope scope_(K_DEC_OTHER, stream);
+    dec_other_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), 4, 16), 128, 0, stream>>>(
+        frames_d, state, shards, t.shards, lists, items, folded);
+  }
+  FVB_LAUNCHED("dec_other_kernel");
   if (wavefront) {
     {
       LaunchScope scope_(K_DEC_RECON, stream);

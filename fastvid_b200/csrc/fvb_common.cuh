@@ -31,9 +31,10 @@ constexpr int kMaxTiles = 1 << 20;
 // pack cost (<= 32 width bytes + 4096*17/8), forced rANS stays below that too.
 constexpr int kMaxRecordBytes = 3 + 32 + (kShardSymbols * 17 + 7) / 8;
 
-// rANS scratch per shard (encoder): symbol table (freq<<16|cum) for the 511
-// symbols, the serialised table, and four byte lanes written back to front.
-constexpr int kRansTableWords = 512;
+// rANS scratch per shard (encoder): symbol table for the 511 symbols (two
+// words each: freq<<16|cum and floor(2^32/freq)), the serialised table, and
+// four byte lanes written back to front.
+constexpr int kRansTableWords = 1024;
 constexpr int kRansSerialBytes = 1024;
 constexpr int kRansLaneBytes = 1792;  // >= 1024 symbols * 12 bits / 8 + 1
 constexpr int kRansScratchBytes = kRansTableWords * 4 + kRansSerialBytes + 4 * kRansLaneBytes;

@@ -36,6 +36,9 @@ __device__ __forceinline__ uint32_t rd32(const uint8_t* p) {
 __device__ __forceinline__ uint64_t rd64(const uint8_t* p) {
   return rd32(p) | (static_cast<uint64_t>(rd32(p + 4)) << 32);
 }
+__device__ __forceinline__ int list_of_mode(int mode) {
+  return mode == kModeOrder0 ? 0 : (mode >= 1 && mode <= 17) ? 1 : mode == 0 ? 2 : 3;
+}
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -43,7 +46,8 @@ __device__ __forceinline__ uint64_t rd64(const uint8_t* p) {
 // (status 11), one thread per tile.
 
 __global__ void dec_parse_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state, int nframes,
-                                 int64_t total_tiles, ShardInfo* __restrict__ shards) {
+                                 int64_t total_tiles, ShardInfo* __restrict__ shards, int64_t total_shards,
+                                 DecodeLists* __restrict__ lists, int32_t* __restrict__ list_items) {
   for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total_tiles;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int fi = frame_of_tile(frames, nframes, t);
@@ -116,123 +120,521 @@ __global__ void dec_parse_kernel(const FrameDesc* __restrict__ frames, FrameStat
       decoded += cnt;
       cursor = bo + bl;
     }
-    if (!ok || decoded != samples || cursor != tile_end) set_status(&st.status, 11);
+    if (!ok || decoded != samples || cursor != tile_end) {
+      set_status(&st.status, 11);
+      continue;
+    }
+    // bin the tile's shards by entropy mode for dec_shards
+    for (int j = 0; j < g.shard_count; ++j) {
+      const int64_t s = f.shard_base + g.first_shard + j;
+      const int list = list_of_mode(shards[s].mode);
+      const int pos = atomicAdd(&lists->count[list], 1);
+      list_items[static_cast<int64_t>(list) * total_shards + pos] = static_cast<int32_t>(s);
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
-// dec_shards: one warp per shard.
+// Entropy decode (decode.cu:222-550).  dec_parse bins shards by mode; then
+//   dec_rans_tables  one thread per rANS shard parses its order-0 table
+//                    serially (decode.cu:456-517) into a table record
+//   dec_rans         a warp takes eight rANS shards: copies their tables into
+//                    shared memory, builds a coarse slot table, and lane 4g+l
+//                    decodes lane l of shard g (decode.cu:530-549)
+//   dec_other        a warp takes eight Rice, zero-run or block shards: Rice
+//                    lane l of shard g on lane 4g+l (decode.cu:297-340),
+//                    zero-run shard g on lane 4g (decode.cu:237-295), block
+//                    shards one after another warp-wide (decode.cu:342-396)
 
-struct DecWarpSmem {
-  uint8_t table[1 << kRansTableLog];
-  uint16_t values[256], freq[256], cum[256];
+constexpr int kGroup = 8;        // shards per warp
+constexpr int kCoarseShift = 3;  // coarse bucket = 8 slots
+
+struct RansTable {
   int32_t lane_start[4], lane_len[4];
-  uint32_t states[4];
+  uint32_t state[4];
   int32_t nsym, valid;
-  int32_t boff[32], bwidth[32];
+  int32_t pad[2];
+  uint2 info[256];  // x: cum | freq << 16, y: (cum + freq) | value << 16 (value as u16, decode.cu:484)
 };
 
-// Rice lane reader with a 64-bit bit buffer (decode.cu:63-125 semantics).
-struct RiceReader {
-  const uint8_t* bytes;
-  int64_t len, bp, pos;
-  uint64_t buf;
-  int nb;
+size_t dec_rans_table_bytes() { return sizeof(RansTable); }
+
+// Sequential reader of a byte range through aligned 32-bit loads.  Only words
+// holding at least one byte of the range are loaded; four are kept in flight
+// ahead of the bit buffer.  Bytes past the range read as zero.
+struct ByteWindow {
+  const uint32_t* words;
+  int64_t next, last;
+  int tail_bytes;
+  uint64_t bits;
+  int nbits;
+  uint32_t q0, q1, q2, q3;
+  int c0, c1, c2, c3;
+
+  // Issues the load of the next word and returns it unmasked; nothing here
+  // waits for the data (bytes past the range are masked off when merged).
+  __device__ uint32_t load_word(int* nb) {
+    const int64_t at = next < last ? next : (last > 0 ? last : 0);
+    const int valid = next < last ? 4 : (next == last ? tail_bytes : 0);
+    const uint32_t w = last >= 0 ? __ldg(words + at) : 0u;
+    ++next;
+    *nb = 8 * valid;
+    return w;
+  }
+  __device__ void init(const uint8_t* p, int64_t len) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const int head = static_cast<int>(a & 3);
+    words = reinterpret_cast<const uint32_t*>(a - head);
+    next = 0;
+    last = len > 0 ? (head + len - 1) >> 2 : -1;
+    tail_bytes = len > 0 ? static_cast<int>((head + len - 1) & 3) + 1 : 0;
+    int nb;
+    const uint32_t w = load_word(&nb);
+    q0 = load_word(&c0);
+    q1 = load_word(&c1);
+    q2 = load_word(&c2);
+    q3 = load_word(&c3);
+    const uint32_t w0 = nb >= 32 ? w : (w & ((1u << nb) - 1u));
+    bits = nb ? (w0 >> (8 * head)) : 0u;
+    nbits = nb ? nb - 8 * head : 0;
+    refill();
+  }
+  __device__ void shift_in() {
+    const uint32_t m0 = c0 >= 32 ? q0 : (q0 & ((1u << c0) - 1u));
+    bits |= static_cast<uint64_t>(m0) << nbits;
+    nbits += c0;
+    q0 = q1;
+    c0 = c1;
+    q1 = q2;
+    c1 = c2;
+    q2 = q3;
+    c2 = c3;
+    q3 = load_word(&c3);
+  }
+  __device__ void refill_once() {
+    if (nbits <= 32) shift_in();
+  }
   __device__ void refill() {
-    while (nb <= 56 && bp < len) {
-      buf |= static_cast<uint64_t>(bytes[bp++]) << nb;
-      nb += 8;
-    }
+    while (nbits <= 32 && c0) shift_in();
   }
-  __device__ bool read(int k, uint32_t maxf, uint32_t* out) {
-    uint32_t q = 0;
-    for (;;) {
-      if (nb == 0) {
-        refill();
-        if (nb == 0) return false;
-      }
-      if (buf == 0) {
-        q += nb;
-        pos += nb;
-        nb = 0;
-        if (q > maxf) return false;
-        continue;
-      }
-      const int z = __ffsll(static_cast<long long>(buf)) - 1;
-      q += z;
-      const int used = z + 1;
-      buf = used == 64 ? 0 : buf >> used;
-      nb -= used;
-      pos += used;
-      if (q > maxf) return false;
-      break;
-    }
-    if (nb < k) refill();
-    if (nb < k) return false;
-    const uint32_t r = k ? static_cast<uint32_t>(buf) & ((1u << k) - 1u) : 0u;
-    buf >>= k;
-    nb -= k;
-    pos += k;
-    const uint64_t v = (static_cast<uint64_t>(q) << k) + r;
-    if (v > maxf) return false;
-    *out = static_cast<uint32_t>(v);
-    return true;
+  __device__ uint32_t byte() {  // next byte (zero past the range)
+    if (nbits < 8) refill();
+    const uint32_t b = static_cast<uint32_t>(bits) & 0xffu;
+    bits >>= 8;
+    nbits -= 8;
+    return b;
   }
 };
 
-__device__ bool read_varint_strict(const uint8_t* body, int64_t len, int64_t* cursor, uint32_t* value) {
-  uint32_t result = 0;
-  int shift = 0;
-  for (int used = 0; used < 5; ++used) {
-    if (*cursor >= len) return false;
-    const uint8_t byte = body[(*cursor)++];
-    if (used == 4 && byte > 0x0f) return false;
-    result |= static_cast<uint32_t>(byte & 0x7f) << shift;
-    if ((byte & 0x80) == 0) {
-      if (varint_len(result) != used + 1) return false;
-      *value = result;
-      return true;
+// Asynchronous 4-byte global -> shared copies (cp.async, sm_80+).
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait2() { asm volatile("cp.async.wait_group 2;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// A lane's byte stream through a private 16-word ring in shared memory, fed
+// by cp.async four words at a time and kept 12-15 words ahead of the read
+// position: reads are shared-memory loads whose data arrived long before.
+// Word w of the aligned range lives in ring slot w & 15; only words holding a
+// byte of the lane are copied (others keep stale bytes, and reading them is
+// an overrun that the byte count check reports).
+struct LaneRing {
+  uint32_t* ring;          // 16 words of shared memory
+  const uint32_t* words;   // aligned base of the lane's bytes
+  int head;                // lane byte 0 = byte `head` of word 0
+  int last;                // last word holding a lane byte (-1: none)
+  int fetched;             // words issued so far (multiple of 4)
+
+  __device__ void fetch4() {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int w = fetched + j;
+      if (w <= last) cp_async4(ring + (w & 15), words + w);
     }
-    shift += 7;
+    cp_async_commit();
+    fetched += 4;
   }
-  return false;
+  __device__ void init(uint32_t* ring_smem, const uint8_t* p, int len) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    head = static_cast<int>(a & 3);
+    words = reinterpret_cast<const uint32_t*>(a - head);
+    ring = ring_smem;
+    last = len > 0 ? (head + len - 1) >> 2 : -1;
+    fetched = 0;
+    fetch4();
+    fetch4();
+    fetch4();
+  }
+  // make the bytes at lane positions cur, cur+1 readable and return them
+  __device__ void read2(int cur, uint32_t& b0, uint32_t& b1) {
+    const int pos = head + cur;
+    if (fetched - (pos >> 2) < 12) fetch4();
+    cp_async_wait2();  // the two newest groups may stay in flight
+    const uint8_t* rb = reinterpret_cast<const uint8_t*>(ring);
+    b0 = rb[pos & 63];
+    b1 = rb[(pos + 1) & 63];
+  }
+};
+
+// Order-0 table of one shard, parsed by one thread (decode.cu:456-517).
+__device__ bool rans_parse_serial(const uint8_t* __restrict__ body, int64_t blen, uint32_t maxf,
+                                  RansTable& t) {
+  ByteWindow r;
+  r.init(body, blen);
+  int64_t cursor = 0;
+  auto varint = [&](uint32_t* value) -> bool {
+    uint32_t result = 0;
+    int shift = 0;
+    for (int used = 0; used < 5; ++used) {
+      if (cursor >= blen) return false;
+      const uint32_t b = r.byte();
+      ++cursor;
+      if (used == 4 && b > 0x0f) return false;
+      result |= (b & 0x7f) << shift;
+      if ((b & 0x80) == 0) {
+        if (varint_len(result) != used + 1) return false;
+        *value = result;
+        return true;
+      }
+      shift += 7;
+    }
+    return false;
+  };
+  if (blen < 1) return false;
+  ++cursor;
+  if (r.byte() != kRansTableLog) return false;
+  uint32_t n = 0;
+  if (!varint(&n) || n == 0 || n > 255) return false;
+  uint32_t prev = 0, assigned = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t delta = 0;
+    if (!varint(&delta) || (i != 0 && delta == 0) || prev + delta > maxf) return false;
+    const uint32_t value = prev + delta;
+    uint32_t fr = (1u << kRansTableLog) - assigned;
+    if (i + 1 != n && !varint(&fr)) return false;
+    // no 32-bit wrap-around: a frequency above 4096 - assigned is rejected
+    // (decode.cu:479-480 would wrap and then overrun its slot table)
+    if (fr == 0 || fr > (1u << kRansTableLog) - assigned ||
+        (i + 1 != n && fr == (1u << kRansTableLog) - assigned))
+      return false;
+    t.info[i] = make_uint2(assigned | (fr << 16), (assigned + fr) | ((value & 0xffffu) << 16));
+    assigned += fr;
+    prev = value;
+  }
+  if (assigned != (1u << kRansTableLog)) return false;
+  // three lane lengths (int in the reference: >= 2^31 ends in status 5
+  // there too), four states, the fourth length implied
+  int64_t total = 0;
+  for (int l = 0; l < 3; ++l) {
+    if (cursor + 4 > blen) return false;
+    uint32_t v = r.byte();
+    v |= r.byte() << 8;
+    v |= r.byte() << 16;
+    v |= r.byte() << 24;
+    cursor += 4;
+    if (v >= (1u << 31)) return false;
+    t.lane_len[l] = static_cast<int32_t>(v);
+    total += v;
+  }
+  if (cursor + 16 > blen) return false;
+  for (int l = 0; l < 4; ++l) {
+    uint32_t v = r.byte();
+    v |= r.byte() << 8;
+    v |= r.byte() << 16;
+    v |= r.byte() << 24;
+    if (v < kRansL) return false;
+    t.state[l] = v;
+  }
+  cursor += 16;
+  const int64_t l3 = blen - cursor - total;
+  if (l3 < 0) return false;
+  t.lane_len[3] = static_cast<int32_t>(l3);
+  for (int l = 0; l < 4; ++l) {
+    t.lane_start[l] = static_cast<int32_t>(cursor);
+    cursor += t.lane_len[l];
+  }
+  t.nsym = static_cast<int32_t>(n);
+  return cursor == blen;
 }
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
-dec_shards_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
-                  const ShardInfo* __restrict__ shards, int64_t total_shards, uint32_t* __restrict__ folded) {
-  __shared__ DecWarpSmem smem_all[kWarpsPerCta];
+__global__ void __launch_bounds__(128)
+dec_rans_tables_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
+                       const ShardInfo* __restrict__ shards, const DecodeLists* __restrict__ lists,
+                       const int32_t* __restrict__ list_items, RansTable* __restrict__ tables) {
+  const int count = lists->count[0];
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
+    const ShardInfo& si = shards[list_items[p]];
+    FrameState& st = state[si.frame];
+    RansTable& t = tables[p];
+    bool ok = false;
+    if (st.status == 0) {  // a failed parse may have left shard records unwritten
+      const FrameDesc& f = frames[si.frame];
+      ok = rans_parse_serial(f.stream + si.offset, si.body, static_cast<uint32_t>(f.max_sample) * 2u, t);
+      if (!ok) set_status(&st.status, 5);
+    }
+    t.valid = ok;
+  }
+}
+
+struct RansShardSm {
+  uint8_t coarse[(1 << kRansTableLog) >> kCoarseShift];  // first symbol of each 8-slot bucket
+  uint2 info[256];
+};
+
+struct RansGroupSm {
+  RansShardSm r[kGroup];
+  uint32_t bitmap[128];
+  uint32_t rings[32][16];  // per-lane byte-stream rings
+  int32_t valid[kGroup];
+};
+
+size_t dec_rans_smem() { return sizeof(RansGroupSm); }
+
+__global__ void __launch_bounds__(32)
+dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
+                const ShardInfo* __restrict__ shards, DecodeLists* __restrict__ lists,
+                const int32_t* __restrict__ list_items, const RansTable* __restrict__ tables,
+                uint32_t* __restrict__ folded) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RansGroupSm& sm = *reinterpret_cast<RansGroupSm*>(smem_raw);
+  const int lane = threadIdx.x;
+  const int my_g = lane >> 2, my_l = lane & 3;
+  const int count = lists->count[0];
+  const int ngroups = (count + kGroup - 1) / kGroup;
+  for (;;) {
+    int g = 0;
+    if (lane == 0) g = atomicAdd(&lists->next_group_rans, 1);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= ngroups) break;
+    const int first = g * kGroup;
+    // tables of the eight shards into shared memory, coarse bucket tables
+    for (int k = 0; k < kGroup; ++k) {
+      const int p = first + k;
+      const bool live = p < count && tables[p].valid;
+      if (lane == 0) sm.valid[k] = live;
+      if (!live) continue;
+      const int n = tables[p].nsym;
+      for (int i = lane; i < n; i += 32) sm.r[k].info[i] = tables[p].info[i];
+      for (int i = lane; i < 128; i += 32) sm.bitmap[i] = 0;
+      __syncwarp();
+      for (int i = 1 + lane; i < n; i += 32) {
+        const uint32_t c = sm.r[k].info[i].x & 0xffffu;
+        atomicOr(&sm.bitmap[c >> 5], 1u << (c & 31));
+      }
+      __syncwarp();
+      uint32_t w[4];
+      int cnt = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        w[j] = sm.bitmap[lane * 4 + j];
+        cnt += __popc(w[j]);
+      }
+      int inc = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += v;
+      }
+      int base = inc - cnt;  // symbol starts before this lane's 128 slots
+      uint32_t* cw = reinterpret_cast<uint32_t*>(sm.r[k].coarse) + lane * 4;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        uint32_t packed = 0;
+#pragma unroll
+        for (int h = 0; h < 4; ++h)  // starts at or before the bucket's first slot
+          packed |= static_cast<uint32_t>(base + __popc(w[j] & ((2u << (8 * h)) - 1u))) << (8 * h);
+        cw[j] = packed;
+        base += __popc(w[j]);
+      }
+      __syncwarp();
+    }
+    __syncwarp();
+    const int p = first + my_g;
+    if (p < count && sm.valid[my_g]) {
+      const ShardInfo& si = shards[list_items[p]];
+      const FrameDesc& f = frames[si.frame];
+      const uint8_t* body = f.stream + si.offset;
+      uint32_t* out = folded + si.sample_base;
+      const int n = si.count;
+      const RansShardSm& rs = sm.r[my_g];
+      uint32_t x = tables[p].state[my_l];
+      const int llen = tables[p].lane_len[my_l];
+      const uint8_t* __restrict__ lb = body + tables[p].lane_start[my_l];
+      int cur = 0;
+      LaneRing ring;
+      ring.init(sm.rings[lane], lb, llen);
+      // The next two bytes are read one step ahead (their positions do not
+      // depend on the state), so the state chain never waits on memory.
+      uint32_t b0, b1;
+      ring.read2(0, b0, b1);
+      // Branch-free step: after x = freq*(x>>12) + slot - cum, x >= 2^11, so
+      // renormalisation reads one byte when x < 2^23 and a second when
+      // x < 2^15; reading past the lane is an error (decode.cu:540-545).
+      for (int idx = my_l; idx < n; idx += 4) {
+        const uint32_t slot = x & ((1u << kRansTableLog) - 1u);
+        int sym = rs.coarse[slot >> kCoarseShift];
+        uint2 e = rs.info[sym];
+        while (slot >= (e.y & 0xffffu)) e = rs.info[++sym];
+        out[idx] = e.y >> 16;
+        x = (e.x >> 16) * (x >> kRansTableLog) + slot - (e.x & 0xffffu);
+        const int nb = (x < kRansL) + (x < (kRansL >> 8));
+        x = nb == 2 ? (x << 16) | (b0 << 8) | b1 : (nb == 1 ? (x << 8) | b0 : x);
+        cur += nb;
+        ring.read2(cur, b0, b1);
+      }
+      cp_async_wait0();
+      if (cur != llen || x != kRansL) set_status(&state[si.frame].status, 5);
+    }
+    __syncwarp();
+  }
+}
+
+struct OtherGroupSm {
+  int32_t boff[32], bwidth[32];
+  int32_t valid;
+};
+
+__global__ void __launch_bounds__(128)
+dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
+                 const ShardInfo* __restrict__ shards, int64_t total_shards, DecodeLists* __restrict__ lists,
+                 const int32_t* __restrict__ list_items, uint32_t* __restrict__ folded) {
+  __shared__ OtherGroupSm sm_all[4];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  DecWarpSmem& sm = smem_all[warp];
-  const int64_t warps_total = static_cast<int64_t>(gridDim.x) * kWarpsPerCta;
-  for (int64_t s = static_cast<int64_t>(blockIdx.x) * kWarpsPerCta + warp; s < total_shards; s += warps_total) {
-    const ShardInfo& si = shards[s];
-    const int fi = si.frame;
-    FrameState& st = state[fi];
-    if (st.status != 0) continue;  // parse failed: shard records may be incomplete
-    const FrameDesc& f = frames[fi];
-    const uint32_t maxf = static_cast<uint32_t>(f.max_sample) * 2u;
-    const int mode = si.mode;
-    const int64_t blen = si.body;
-    const int64_t n = si.count;
-    const uint8_t* __restrict__ body = f.stream + si.offset;
-    uint32_t* __restrict__ out = folded + si.sample_base;
-    if (mode == 0) {
-      // zero-run varints (decode.cu:237-295)
-      if (lane == 0) {
+  OtherGroupSm& sm = sm_all[warp];
+  const int my_g = lane >> 2, my_l = lane & 3;
+  int ngroups[3], total_groups = 0;
+  for (int l = 0; l < 3; ++l) {
+    ngroups[l] = (lists->count[l + 1] + kGroup - 1) / kGroup;
+    total_groups += ngroups[l];
+  }
+  for (;;) {
+    int g = 0;
+    if (lane == 0) g = atomicAdd(&lists->next_group, 1);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= total_groups) break;
+    int list = 0;
+    while (g >= ngroups[list]) {
+      g -= ngroups[list];
+      ++list;
+    }
+    ++list;  // 1 Rice, 2 zero-run, 3 block pack
+    const int first = g * kGroup;
+    const int count = lists->count[list];
+    const int32_t* items = list_items + static_cast<int64_t>(list) * total_shards;
+    const int64_t s_mine = (first + my_g < count) ? items[first + my_g] : -1;
+    bool live = false;
+    int fi = 0, mode = 0, n = 0;
+    int64_t blen = 0;
+    const uint8_t* body = nullptr;
+    uint32_t* out = nullptr;
+    uint32_t maxf = 0;
+    if (s_mine >= 0) {
+      const ShardInfo& si = shards[s_mine];
+      fi = si.frame;
+      live = state[fi].status == 0;  // a failed parse may have left shard records unwritten
+      mode = si.mode;
+      n = si.count;
+      blen = si.body;
+      body = frames[fi].stream + si.offset;
+      out = folded + si.sample_base;
+      maxf = static_cast<uint32_t>(frames[fi].max_sample) * 2u;
+    }
+    if (list == 1) {
+      // ---- Rice ---------------------------------------------------------------
+      if (s_mine >= 0 && live) {
+        const int lc = n < 4 ? n : 4;
+        const int64_t table = static_cast<int64_t>(lc - 1) * 4;
+        if (table > blen) {
+          if (my_l == 0) set_status(&state[fi].status, 2);
+        } else if (my_l < lc) {
+          int64_t loff = table;
+          for (int i = 0; i < my_l; ++i) loff += rd32(body + i * 4);
+          const int64_t llen = my_l + 1 < lc ? static_cast<int64_t>(rd32(body + my_l * 4)) : blen - loff;
+          bool ok = !(loff > blen || llen < 0 || llen > blen - loff);
+          if (ok) {
+            const int k = mode - 1;
+            const uint32_t rmask = k ? (1u << k) - 1u : 0u;
+            ByteWindow win;
+            win.init(body + loff, llen);
+            int64_t pos = 0;
+            for (int idx = my_l; idx < n && ok; idx += lc) {
+              uint32_t q = 0;
+              for (;;) {
+                if (win.nbits == 0) {
+                  win.refill();
+                  if (win.nbits == 0) {
+                    ok = false;
+                    break;
+                  }
+                }
+                if (win.bits == 0) {
+                  q += win.nbits;
+                  pos += win.nbits;
+                  win.nbits = 0;
+                  if (q > maxf) {
+                    ok = false;
+                    break;
+                  }
+                  continue;
+                }
+                const int z = __ffsll(static_cast<long long>(win.bits)) - 1;
+                q += z;
+                const int used = z + 1;
+                win.bits = used == 64 ? 0 : win.bits >> used;
+                win.nbits -= used;
+                pos += used;
+                if (q > maxf) ok = false;
+                break;
+              }
+              if (!ok) break;
+              if (win.nbits < k) win.refill();
+              if (win.nbits < k) {
+                ok = false;
+                break;
+              }
+              const uint32_t r = static_cast<uint32_t>(win.bits) & rmask;
+              win.bits >>= k;
+              win.nbits -= k;
+              pos += k;
+              const uint64_t v = (static_cast<uint64_t>(q) << k) + r;
+              if (v > maxf) {
+                ok = false;
+                break;
+              }
+              out[idx] = static_cast<uint32_t>(v);
+              if (win.nbits <= 32) win.refill();
+            }
+            if (ok) {
+              const int64_t used = (pos + 7) / 8;
+              if (used != llen) ok = false;
+              else if ((pos & 7) != 0) {
+                const uint8_t mask = static_cast<uint8_t>(~((1u << (pos & 7)) - 1u));
+                if (body[loff + used - 1] & mask) ok = false;
+              }
+            }
+          }
+          if (!ok) set_status(&state[fi].status, 2);
+        }
+      }
+    } else if (list == 2) {
+      // ---- zero-run -----------------------------------------------------------
+      if (my_l == 0 && s_mine >= 0 && live) {
         int64_t cursor = 0, produced = 0;
-        int err = 0;
+        bool err = false;
         while (produced < n && !err) {
           uint32_t token = 0;
           int shift = 0, used = 0;
           for (;;) {
             if (cursor >= blen || used == 5) {
-              err = 1;
+              err = true;
               break;
             }
             const uint8_t byte = body[cursor++];
             if (used == 4 && byte > 0x0f) {
-              err = 1;
+              err = true;
               break;
             }
             token |= static_cast<uint32_t>(byte & 0x7f) << shift;
@@ -242,244 +644,153 @@ dec_shards_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__
           }
           if (err) break;
           if (used != varint_len(token)) {
-            err = 1;
+            err = true;
             break;
           }
           if ((token & 1) == 0) {
             const int64_t run = static_cast<int64_t>(token / 2) + 1;
             if (run > n - produced) {
-              err = 1;
+              err = true;
               break;
             }
             for (int64_t i = 0; i < run; ++i) out[produced++] = 0;
           } else {
             const uint32_t value = (token + 1) / 2;
             if (value == 0 || value > maxf) {
-              err = 1;
+              err = true;
               break;
             }
             out[produced++] = value;
           }
         }
-        if (err || cursor != blen) set_status(&st.status, 1);
+        if (err || cursor != blen) set_status(&state[fi].status, 1);
       }
-    } else if (mode >= 1 && mode <= 17) {
-      // Rice lanes (decode.cu:297-340)
-      const int lc = static_cast<int>(n < 4 ? n : 4);
-      const int64_t table = static_cast<int64_t>(lc - 1) * 4;
-      if (table > blen) {
-        if (lane == 0) set_status(&st.status, 2);
-      } else if (lane < lc) {
-        int64_t loff = table;
-        for (int i = 0; i < lane; ++i) loff += rd32(body + i * 4);
-        const int64_t llen = lane + 1 < lc ? static_cast<int64_t>(rd32(body + lane * 4)) : blen - loff;
-        bool ok = !(loff > blen || llen < 0 || llen > blen - loff);
-        if (ok) {
-          RiceReader rr{body + loff, llen, 0, 0, 0ull, 0};
-          const int k = mode - 1;
-          for (int64_t idx = lane; idx < n; idx += lc) {
-            uint32_t v;
-            if (!rr.read(k, maxf, &v)) {
-              ok = false;
-              break;
-            }
-            out[idx] = v;
-          }
-          if (ok) {
-            const int64_t used = (rr.pos + 7) / 8;
-            if (used != llen) ok = false;
-            else if ((rr.pos & 7) != 0) {
-              const uint8_t mask = static_cast<uint8_t>(~((1u << (rr.pos & 7)) - 1u));
-              if (body[loff + used - 1] & mask) ok = false;
-            }
-          }
-        }
-        if (!ok) set_status(&st.status, 2);
-      }
-    } else if (mode == 18) {
-      // block pack (decode.cu:342-396): walk the width bytes, then decode
-      // the blocks warp-wide
-      const int nblk = static_cast<int>((n + kBlockSymbols - 1) / kBlockSymbols);
-      const int maxw = 32 - __clz(maxf);
-      if (lane == 0) {
-        int64_t cursor = 0;
-        int ok = 1;
-        for (int b = 0; b < nblk; ++b) {
-          if (cursor >= blen) {
-            ok = 0;
-            break;
-          }
-          const int w = body[cursor++];
-          if (w > maxw) {
-            ok = 0;
-            break;
-          }
-          const int64_t nb = min(static_cast<int64_t>(kBlockSymbols), n - static_cast<int64_t>(b) * kBlockSymbols);
-          const int64_t pay = (nb * w + 7) / 8;
-          if (pay > blen - cursor) {
-            ok = 0;
-            break;
-          }
-          sm.boff[b] = static_cast<int32_t>(cursor);
-          sm.bwidth[b] = w;
-          // padding bits of the block's last byte must be zero
-          const int64_t bits = nb * w;
-          if ((bits & 7) != 0) {
-            const uint8_t mask = static_cast<uint8_t>(~((1u << (bits & 7)) - 1u));
-            if (body[cursor + pay - 1] & mask) {
+    } else {
+      // ---- block pack: the warp takes the shards one after another ------------
+      for (int k = 0; k < kGroup; ++k) {
+        const int64_t sk = __shfl_sync(kFull, s_mine, 4 * k);
+        if (sk < 0) continue;
+        const bool lk = __shfl_sync(kFull, live, 4 * k);
+        if (!lk) continue;
+        const int nk = __shfl_sync(kFull, n, 4 * k);
+        const int64_t bk = __shfl_sync(kFull, blen, 4 * k);
+        const int fk = __shfl_sync(kFull, fi, 4 * k);
+        const uint32_t mk = __shfl_sync(kFull, maxf, 4 * k);
+        const uint8_t* bodyk = reinterpret_cast<const uint8_t*>(__shfl_sync(kFull, reinterpret_cast<uintptr_t>(body), 4 * k));
+        uint32_t* outk = reinterpret_cast<uint32_t*>(__shfl_sync(kFull, reinterpret_cast<uintptr_t>(out), 4 * k));
+        const int nblk = (nk + kBlockSymbols - 1) / kBlockSymbols;
+        const int maxw = 32 - __clz(mk);
+        if (lane == 0) {
+          int64_t cursor = 0;
+          int ok = 1;
+          for (int b = 0; b < nblk; ++b) {
+            if (cursor >= bk) {
               ok = 0;
               break;
             }
-          }
-          cursor += pay;
-        }
-        if (ok && cursor != blen) ok = 0;
-        sm.valid = ok;
-        if (!ok) set_status(&st.status, 3);
-      }
-      __syncwarp();
-      if (sm.valid) {
-        int bad = 0;
-        for (int b = 0; b < nblk; ++b) {
-          const int w = sm.bwidth[b];
-          const uint8_t* pay = body + sm.boff[b];
-          const int nb = static_cast<int>(min(static_cast<int64_t>(kBlockSymbols), n - static_cast<int64_t>(b) * kBlockSymbols));
-          for (int i = lane; i < nb; i += 32) {
-            uint32_t v = 0;
-            if (w) {
-              const int64_t bit = static_cast<int64_t>(i) * w;
-              const int64_t byte0 = bit >> 3;
-              const int64_t last = (bit + w - 1) >> 3;
-              uint64_t acc = 0;
-              for (int64_t j = byte0; j <= last; ++j) acc |= static_cast<uint64_t>(pay[j]) << (8 * (j - byte0));
-              v = static_cast<uint32_t>((acc >> (bit & 7)) & ((w == 32) ? 0xffffffffull : ((1ull << w) - 1)));
+            const int w = bodyk[cursor++];
+            if (w > maxw) {
+              ok = 0;
+              break;
             }
-            if (v > maxf) bad = 1;
-            out[static_cast<int64_t>(b) * kBlockSymbols + i] = v;
-          }
-        }
-        if (__any_sync(kFull, bad) && lane == 0) set_status(&st.status, 3);
-      }
-      __syncwarp();
-    } else if (mode == kModeOrder0) {
-      // order-0 rANS (decode.cu:428-550)
-      if (lane == 0) {
-        int valid = 1;
-        int64_t cursor = 0;
-        if (blen < 1 || body[cursor++] != kRansTableLog) valid = 0;
-        uint32_t nsym = 0;
-        if (valid && !read_varint_strict(body, blen, &cursor, &nsym)) valid = 0;
-        if (nsym == 0 || nsym > 255) valid = 0;
-        uint32_t prev = 0, assigned = 0;
-        for (uint32_t i = 0; valid && i < nsym; ++i) {
-          uint32_t delta = 0;
-          if (!read_varint_strict(body, blen, &cursor, &delta) || (i != 0 && delta == 0) || prev + delta > maxf) {
-            valid = 0;
-            break;
-          }
-          const uint32_t value = prev + delta;
-          uint32_t fr = (1u << kRansTableLog) - assigned;
-          if (i + 1 != nsym && !read_varint_strict(body, blen, &cursor, &fr)) {
-            valid = 0;
-            break;
-          }
-          if (fr == 0 || assigned + fr > (1u << kRansTableLog) ||
-              (i + 1 != nsym && assigned + fr == (1u << kRansTableLog))) {
-            valid = 0;
-            break;
-          }
-          sm.values[i] = static_cast<uint16_t>(value);
-          sm.freq[i] = static_cast<uint16_t>(fr);
-          sm.cum[i] = static_cast<uint16_t>(assigned);
-          assigned += fr;
-          prev = value;
-        }
-        if (assigned != (1u << kRansTableLog)) valid = 0;
-        // lane lengths: the reference keeps them as int; any length >= 2^31
-        // or a negative fourth length ends in status 5 there as well.
-        int64_t total = 0;
-        for (int l = 0; valid && l < 3; ++l) {
-          if (cursor + 4 > blen) {
-            valid = 0;
-          } else {
-            const int64_t ll = rd32(body + cursor);
-            if (ll >= (1ll << 31)) valid = 0;
-            sm.lane_len[l] = static_cast<int32_t>(ll);
-            total += ll;
-            cursor += 4;
-          }
-        }
-        if (valid && cursor + 16 > blen) valid = 0;
-        for (int l = 0; valid && l < 4; ++l) {
-          sm.states[l] = rd32(body + cursor + l * 4);
-          if (sm.states[l] < kRansL) valid = 0;
-        }
-        if (valid) {
-          cursor += 16;
-          const int64_t l3 = blen - cursor - total;
-          if (l3 < 0) valid = 0;
-          sm.lane_len[3] = static_cast<int32_t>(l3);
-          for (int l = 0; valid && l < 4; ++l) {
-            sm.lane_start[l] = static_cast<int32_t>(cursor);
-            cursor += sm.lane_len[l];
-          }
-          if (valid && cursor != blen) valid = 0;
-        }
-        sm.nsym = static_cast<int32_t>(nsym);
-        sm.valid = valid;
-        if (!valid) set_status(&st.status, 5);
-      }
-      __syncwarp();
-      if (sm.valid) {
-        for (int sym = 0; sym < sm.nsym; ++sym) {
-          const int b = sm.cum[sym], e = b + sm.freq[sym];
-          for (int slot = b + lane; slot < e; slot += 32) sm.table[slot] = static_cast<uint8_t>(sym);
-        }
-        __syncwarp();
-        if (lane < 4) {
-          uint32_t x = sm.states[lane];
-          const uint8_t* lb = body + sm.lane_start[lane];
-          const int llen = sm.lane_len[lane];
-          int cur = 0;
-          bool ok = true;
-          for (int64_t idx = lane; idx < n; idx += 4) {
-            const uint32_t slot = x & ((1u << kRansTableLog) - 1u);
-            const int sym = sm.table[slot];
-            out[idx] = sm.values[sym];
-            x = static_cast<uint32_t>(sm.freq[sym]) * (x >> kRansTableLog) + slot - sm.cum[sym];
-            while (x < kRansL) {
-              if (cur >= llen) {
-                ok = false;
+            const int64_t nb = min(static_cast<int64_t>(kBlockSymbols), static_cast<int64_t>(nk) - static_cast<int64_t>(b) * kBlockSymbols);
+            const int64_t pay = (nb * w + 7) / 8;
+            if (pay > bk - cursor) {
+              ok = 0;
+              break;
+            }
+            sm.boff[b] = static_cast<int32_t>(cursor);
+            sm.bwidth[b] = w;
+            const int64_t bits = nb * w;
+            if ((bits & 7) != 0) {
+              const uint8_t mask = static_cast<uint8_t>(~((1u << (bits & 7)) - 1u));
+              if (bodyk[cursor + pay - 1] & mask) {
+                ok = 0;
                 break;
               }
-              x = (x << 8) | lb[cur++];
             }
-            if (!ok) break;
+            cursor += pay;
           }
-          if (!ok || cur != llen || x != kRansL) set_status(&st.status, 5);
+          if (ok && cursor != bk) ok = 0;
+          sm.valid = ok;
+          if (!ok) set_status(&state[fk].status, 3);
         }
+        __syncwarp();
+        if (sm.valid) {
+          int bad = 0;
+          for (int b = 0; b < nblk; ++b) {
+            const int w = sm.bwidth[b];
+            const uint8_t* pay = bodyk + sm.boff[b];
+            const int nb = min(kBlockSymbols, nk - b * kBlockSymbols);
+            for (int i = lane; i < nb; i += 32) {
+              uint32_t v = 0;
+              if (w) {
+                const int64_t bit = static_cast<int64_t>(i) * w;
+                const int64_t byte0 = bit >> 3;
+                const int64_t lastb = (bit + w - 1) >> 3;
+                uint64_t acc = 0;
+                for (int64_t j = byte0; j <= lastb; ++j) acc |= static_cast<uint64_t>(pay[j]) << (8 * (j - byte0));
+                v = static_cast<uint32_t>((acc >> (bit & 7)) & ((1ull << w) - 1));
+              }
+              if (v > mk) bad = 1;
+              outk[static_cast<int64_t>(b) * kBlockSymbols + i] = v;
+            }
+          }
+          if (__any_sync(kFull, bad) && lane == 0) set_status(&state[fk].status, 3);
+        }
+        __syncwarp();
       }
-      __syncwarp();
-    } else {
-      if (lane == 0) set_status(&st.status, 4);
     }
   }
 }
+
 
 // ---------------------------------------------------------------------------
 // dec_reconstruct: warp per tile, lane = row of a 32-row band, column c of
 // row i at step c + i; the folded tile streams through a 64-column ring and
 // the reconstruction is flushed to the output plane 32 columns at a time.
 
+// Mirror of enc_tile_fast: the folded residuals stream in through a skewed
+// 64-column ring, the reconstruction goes out through another and is flushed
+// to the output plane 32 columns at a time (decode.cu:552-606).
+
 struct RecWarpSmem {
-  uint32_t fold[32 * kFoldStride];
-  uint16_t out[32 * kSrcStride];
-  uint16_t carry[kFastMaxW];
+  uint32_t fold[32 * kFoldStride];  // folded-residual ring (u32, skewed)
+  uint16_t out[32 * kSrcStride];    // reconstruction ring (u16, skewed)
+  uint16_t carry[kFastMaxW + 128];  // row above the band, column c at index c + 32
 };
 
 size_t dec_reconstruct_smem() { return sizeof(RecWarpSmem) * kWarpsPerCta; }
 
-template <bool MED>
+template <bool MED, bool STEP1, bool EDGE>
+__device__ __forceinline__ void rec_block(RecWarpSmem& sm, int lane, int t0, int W, int32_t maxs, int32_t step,
+                                          bool band0, int32_t& rec, int32_t& a_prev) {
+  const uint32_t* frow = sm.fold + lane * kFoldStride + (t0 & 32);
+  uint16_t* orow = sm.out + lane * kSrcStride + (t0 & 32);
+  uint16_t* crow = sm.carry + 32 - lane + t0;
+#pragma unroll
+  for (int u = 0; u < 32; ++u) {
+    const uint32_t fv = frow[u];
+    int32_t a = __shfl_up_sync(0xffffffffu, rec, 1);
+    const int32_t above0 = crow[u];
+    if (lane == 0) a = band0 ? 0 : above0;
+    const int32_t pred = MED ? predict_med(rec, a, a_prev) : predict_grad(rec, a, a_prev, maxs);
+    const int32_t q = unzigzag(fv);
+    int32_t rn = max(0, min(maxs, STEP1 ? pred + q : pred + q * step));
+    if (EDGE) {
+      const int c = t0 + u - lane;
+      if (c < 0) rn = 0;
+      if (lane == 31 && c >= 0 && c < W) crow[u] = static_cast<uint16_t>(rn);
+    } else {
+      if (lane == 31) crow[u] = static_cast<uint16_t>(rn);
+    }
+    orow[u] = static_cast<uint16_t>(rn);
+    a_prev = a;
+    rec = rn;
+  }
+}
+
+template <bool MED, bool STEP1>
 __device__ void rec_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step,
                               const uint32_t* __restrict__ ftile, RecWarpSmem& sm, int lane) {
   uint16_t* __restrict__ plane = f.dst[g.plane];
@@ -487,80 +798,53 @@ __device__ void rec_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
   const int W = g.w, H = g.h;
   const int32_t maxs = f.max_sample;
   const int nchunks = (W + 31) >> 5;
-  const int nsteps = W + 31;
-  const int nblocks = (nsteps + 31) >> 5;
+  const int nblocks = (W + 31 + 31) >> 5;
   for (int band = 0; band * 32 < H; ++band) {
     const int band_rows = min(32, H - band * 32);
-    uint16_t* __restrict__ orow = plane + static_cast<int64_t>(g.y + band * 32) * pitch + g.x;
-    const uint32_t* __restrict__ frow = ftile + static_cast<int64_t>(band * 32) * W;
+    uint16_t* __restrict__ orows = plane + static_cast<int64_t>(g.y + band * 32) * pitch + g.x;
+    const uint32_t* __restrict__ frows = ftile + static_cast<int64_t>(band * 32) * W;
     uint32_t pf[32];
+    auto load_chunk = [&](int k) {
+      const int col = k * 32 + lane;
 #pragma unroll
-    for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && lane < W) ? frow[static_cast<int64_t>(r) * W + lane] : 0u;
+      for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && col < W) ? __ldg(frows + static_cast<int64_t>(r) * W + col) : 0u;
+    };
+    auto store_chunk = [&](int k) {
+      const int pj = k * 32 + lane;
 #pragma unroll
-    for (int r = 0; r < 32; ++r) sm.fold[r * kFoldStride + lane] = pf[r];
-#pragma unroll
-    for (int r = 0; r < 32; ++r) {
-      const int col = 32 + lane;
-      pf[r] = (r < band_rows && col < W) ? frow[static_cast<int64_t>(r) * W + col] : 0u;
-    }
+      for (int r = 0; r < 32; ++r) sm.fold[r * kFoldStride + ((pj + r) & 63)] = pf[r];
+    };
+    auto flush_chunk = [&](int k) {
+      const int col = k * 32 + lane;
+      if (col < W) {
+        for (int r = 0; r < band_rows; ++r)
+          orows[static_cast<int64_t>(r) * pitch + col] = sm.out[r * kSrcStride + ((col + r) & 63)];
+      }
+    };
+    load_chunk(0);
+    store_chunk(0);
+    if (nchunks > 1) load_chunk(1);
     __syncwarp();
     int32_t rec = 0, a_prev = 0;
+    const bool band0 = band == 0;
     for (int blk = 0; blk < nblocks; ++blk) {
       if (blk > 0) {
-        if (blk < nchunks) {
-          const int slot = (blk & 1) * 32;
-#pragma unroll
-          for (int r = 0; r < 32; ++r) sm.fold[r * kFoldStride + slot + lane] = pf[r];
-        }
+        if (blk < nchunks) store_chunk(blk);
         __syncwarp();
-        if (blk >= 2 && blk - 2 < nchunks) {
-          const int j = blk - 2;
-          const int col = j * 32 + lane;
-          const int slot = (j & 1) * 32;
-          if (col < W) {
-            for (int r = 0; r < band_rows; ++r) orow[static_cast<int64_t>(r) * pitch + col] = sm.out[r * kSrcStride + slot + lane];
-          }
-        }
-        if (blk + 1 < nchunks) {
-          const int col = (blk + 1) * 32 + lane;
-#pragma unroll
-          for (int r = 0; r < 32; ++r)
-            pf[r] = (r < band_rows && col < W) ? frow[static_cast<int64_t>(r) * W + col] : 0u;
-        }
+        if (blk >= 2 && blk - 2 < nchunks) flush_chunk(blk - 2);
+        if (blk + 1 < nchunks) load_chunk(blk + 1);
       }
       const int t0 = blk * 32;
-#pragma unroll 4
-      for (int u = 0; u < 32; ++u) {
-        const int c = t0 + u - lane;
-        const bool in = (c >= 0) && (c < W);
-        const int cc = c & 63;
-        const uint32_t fv = sm.fold[lane * kFoldStride + cc];
-        int32_t a = __shfl_up_sync(kFull, rec, 1);
-        if (lane == 0) a = (band > 0 && in) ? static_cast<int32_t>(sm.carry[c]) : 0;
-        const int32_t pred = MED ? predict_med(rec, a, a_prev) : predict_grad(rec, a, a_prev, maxs);
-        int32_t rn = max(0, min(maxs, pred + unzigzag(fv) * step));
-        if (c < 0) rn = 0;
-        if (in) {
-          sm.out[lane * kSrcStride + cc] = static_cast<uint16_t>(rn);
-          if (lane == 31) sm.carry[c] = static_cast<uint16_t>(rn);
-        }
-        a_prev = a;
-        rec = rn;
-      }
+      if (t0 < 31 || t0 + 31 >= W) rec_block<MED, STEP1, true>(sm, lane, t0, W, maxs, step, band0, rec, a_prev);
+      else rec_block<MED, STEP1, false>(sm, lane, t0, W, maxs, step, band0, rec, a_prev);
     }
     __syncwarp();
-    for (int j = max(0, nblocks - 2); j < nchunks; ++j) {
-      const int col = j * 32 + lane;
-      const int slot = (j & 1) * 32;
-      if (col < W) {
-        for (int r = 0; r < band_rows; ++r) orow[static_cast<int64_t>(r) * pitch + col] = sm.out[r * kSrcStride + slot + lane];
-      }
-    }
+    for (int j = max(0, nblocks - 2); j < nchunks; ++j) flush_chunk(j);
     __syncwarp();
   }
 }
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
 dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state, int nframes,
                        int64_t total_tiles, const uint32_t* __restrict__ folded, int* __restrict__ queue) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -577,8 +861,13 @@ dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* _
     const TileGeo g = tile_geo(f, t - f.tile_base);
     if (g.w > kFastMaxW) continue;
     const uint32_t* ftile = folded + f.sample_base + g.sample_base;
-    if (f.use_med0) rec_tile_fast<true>(f, g, f.step0, ftile, sm, lane);
-    else rec_tile_fast<false>(f, g, f.step0, ftile, sm, lane);
+    if (f.use_med0) {
+      if (f.step0 == 1) rec_tile_fast<true, true>(f, g, 1, ftile, sm, lane);
+      else rec_tile_fast<true, false>(f, g, f.step0, ftile, sm, lane);
+    } else {
+      if (f.step0 == 1) rec_tile_fast<false, true>(f, g, 1, ftile, sm, lane);
+      else rec_tile_fast<false, false>(f, g, f.step0, ftile, sm, lane);
+    }
   }
 }
 

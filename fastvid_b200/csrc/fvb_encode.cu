@@ -42,115 +42,122 @@ __device__ __forceinline__ int32_t div_step(uint32_t n, uint32_t magic) {
 // ---------------------------------------------------------------------------
 // enc_predict
 
+// Warp-per-tile register wavefront over 32-row bands.  Lane i holds row i of
+// the band and processes column c = t - i at step t, so its left and
+// upper-left neighbours are its own previous values and its upper neighbour
+// is lane i-1's previous reconstruction (one shuffle); lane 0 reads the row
+// above the band from the carry row written by lane 31 of the previous band.
+// Source and output stream through two 64-column shared-memory rings in a
+// skewed layout -- row r keeps column c at position (c + r) & 63 -- so at
+// step t every lane touches position t & 63: one uniform offset, folded into
+// the instruction's immediate inside each unrolled 32-step block.  Blocks in
+// which every lane's column lies inside the tile run without predicates.
+
 struct EncWarpSmem {
-  uint16_t src[32 * kSrcStride];   // source ring, 64 columns
-  uint32_t fold[32 * kFoldStride]; // folded ring, 64 columns
-  uint16_t carry[kFastMaxW];       // reconstruction of the row above the band
+  uint16_t src[32 * kSrcStride];    // source ring (u16, skewed)
+  uint32_t fold[32 * kFoldStride];  // folded-residual ring (u32, skewed)
+  uint16_t carry[kFastMaxW + 128];  // row above the band, column c at index c + 32
 };
+
+template <bool MED, bool STEP1, bool EDGE>
+__device__ __forceinline__ void enc_block(EncWarpSmem& sm, int lane, int t0, int W,
+                                          int32_t maxs, int32_t step, int32_t half, uint32_t magic, bool band0,
+                                          int32_t& rec, int32_t& a_prev) {
+  const uint16_t* srow = sm.src + lane * kSrcStride + (t0 & 32);
+  uint32_t* frow = sm.fold + lane * kFoldStride + (t0 & 32);
+  uint16_t* crow = sm.carry + 32 - lane + t0;  // carry index (t - lane) + 32
+#pragma unroll
+  for (int u = 0; u < 32; ++u) {
+    const int32_t s = srow[u];
+    int32_t a = __shfl_up_sync(0xffffffffu, rec, 1);
+    const int32_t above0 = crow[u];
+    if (lane == 0) a = band0 ? 0 : above0;
+    const int32_t pred = MED ? predict_med(rec, a, a_prev) : predict_grad(rec, a, a_prev, maxs);
+    const int32_t res = s - pred;
+    int32_t q, rn;
+    if (STEP1) {
+      q = res;
+      rn = min(s, maxs);
+    } else {
+      const int32_t mag = static_cast<int32_t>(__umulhi(static_cast<uint32_t>(abs(res) + half), magic));
+      q = res < 0 ? -mag : mag;
+      rn = max(0, min(maxs, pred + q * step));
+    }
+    if (EDGE) {
+      const int c = t0 + u - lane;
+      if (c < 0) rn = 0;  // left of the tile: zero left/upper-left for column 0
+      if (lane == 31 && c >= 0 && c < W) crow[u] = static_cast<uint16_t>(rn);
+    } else {
+      if (lane == 31) crow[u] = static_cast<uint16_t>(rn);
+    }
+    frow[u] = zigzag(q);
+    a_prev = a;
+    rec = rn;
+  }
+}
 
 template <bool MED, bool STEP1>
 __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step, uint32_t magic,
-                              uint32_t* __restrict__ folded_tile, EncWarpSmem& sm, int lane,
-                              int32_t& bad) {
+                              uint32_t* __restrict__ folded_tile, EncWarpSmem& sm, int lane, int32_t& bad) {
   const uint16_t* __restrict__ plane = f.src[g.plane];
   const int64_t pitch = f.src_pitch[g.plane];
   const int W = g.w, H = g.h;
   const int32_t maxs = f.max_sample;
   const int32_t half = step >> 1;
   const int nchunks = (W + 31) >> 5;
-  const int nsteps = W + 31;
-  const int nblocks = (nsteps + 31) >> 5;
+  const int nblocks = (W + 31 + 31) >> 5;
+  uint32_t vmax = 0;
   for (int band = 0; band * 32 < H; ++band) {
     const int band_rows = min(32, H - band * 32);
-    const bool row_ok = lane < band_rows;
     const uint16_t* __restrict__ rows = plane + static_cast<int64_t>(g.y + band * 32) * pitch + g.x;
-    uint32_t* __restrict__ frow = folded_tile + static_cast<int64_t>(band * 32) * W;
+    uint32_t* __restrict__ frows = folded_tile + static_cast<int64_t>(band * 32) * W;
     uint32_t pf[32];
-    // chunk 0 -> ring slot 0
+    auto load_chunk = [&](int k) {
+      const int col = k * 32 + lane;
 #pragma unroll
-    for (int r = 0; r < 32; ++r) {
-      const int col = lane;
-      pf[r] = (r < band_rows && col < W) ? rows[static_cast<int64_t>(r) * pitch + col] : 0u;
-    }
-#pragma unroll
-    for (int r = 0; r < 32; ++r) sm.src[r * kSrcStride + lane] = static_cast<uint16_t>(pf[r]);
-    // prefetch chunk 1
-#pragma unroll
-    for (int r = 0; r < 32; ++r) {
-      const int col = 32 + lane;
-      pf[r] = (r < band_rows && col < W) ? rows[static_cast<int64_t>(r) * pitch + col] : 0u;
-    }
-    __syncwarp();
-    int32_t rec = 0, a_prev = 0;
-    for (int blk = 0; blk < nblocks; ++blk) {
-      if (blk > 0) {
-        // store chunk blk (prefetched), flush chunk blk-2, prefetch chunk blk+1
-        if (blk < nchunks) {
-          const int slot = (blk & 1) * 32;
-#pragma unroll
-          for (int r = 0; r < 32; ++r) sm.src[r * kSrcStride + slot + lane] = static_cast<uint16_t>(pf[r]);
-        }
-        __syncwarp();
-        if (blk >= 2 && blk - 2 < nchunks) {
-          const int j = blk - 2;
-          const int col = j * 32 + lane;
-          const int slot = (j & 1) * 32;
-          if (col < W) {
-            for (int r = 0; r < band_rows; ++r)
-              frow[static_cast<int64_t>(r) * W + col] = sm.fold[r * kFoldStride + slot + lane];
-          }
-        }
-        if (blk + 1 < nchunks) {
-          const int col = (blk + 1) * 32 + lane;
-#pragma unroll
-          for (int r = 0; r < 32; ++r)
-            pf[r] = (r < band_rows && col < W) ? rows[static_cast<int64_t>(r) * pitch + col] : 0u;
-        }
+      for (int r = 0; r < 32; ++r) {
+        pf[r] = (r < band_rows && col < W) ? rows[static_cast<int64_t>(r) * pitch + col] : 0u;
+        vmax = max(vmax, pf[r]);
       }
-      const int t0 = blk * 32;
-#pragma unroll 4
-      for (int u = 0; u < 32; ++u) {
-        const int c = t0 + u - lane;
-        const bool in = (c >= 0) && (c < W);
-        const int cc = c & 63;
-        const int32_t s = sm.src[lane * kSrcStride + cc];
-        int32_t a = __shfl_up_sync(kFull, rec, 1);
-        if (lane == 0) a = (band > 0 && in) ? static_cast<int32_t>(sm.carry[c]) : 0;
-        const int32_t pred = MED ? predict_med(rec, a, a_prev) : predict_grad(rec, a, a_prev, maxs);
-        const int32_t res = s - pred;
-        int32_t q, rn;
-        if (STEP1) {
-          q = res;
-          rn = min(s, maxs);
-        } else {
-          const int32_t mag = div_step(static_cast<uint32_t>(abs(res) + half), magic);
-          q = res < 0 ? -mag : mag;
-          rn = max(0, min(maxs, pred + q * step));
-        }
-        if (c < 0) rn = 0;
-        if (in) {
-          sm.fold[lane * kFoldStride + cc] = zigzag(q);
-          if (row_ok && s > maxs) bad = 1;
-          if (lane == 31) sm.carry[c] = static_cast<uint16_t>(rn);
-        }
-        a_prev = a;
-        rec = rn;
-      }
-    }
-    __syncwarp();
-    for (int j = max(0, nblocks - 2); j < nchunks; ++j) {
-      const int col = j * 32 + lane;
-      const int slot = (j & 1) * 32;
+    };
+    auto store_chunk = [&](int k) {
+      const int pj = k * 32 + lane;
+#pragma unroll
+      for (int r = 0; r < 32; ++r) sm.src[r * kSrcStride + ((pj + r) & 63)] = static_cast<uint16_t>(pf[r]);
+    };
+    auto flush_chunk = [&](int k) {
+      const int col = k * 32 + lane;
       if (col < W) {
         for (int r = 0; r < band_rows; ++r)
-          frow[static_cast<int64_t>(r) * W + col] = sm.fold[r * kFoldStride + slot + lane];
+          frows[static_cast<int64_t>(r) * W + col] = sm.fold[r * kFoldStride + ((col + r) & 63)];
       }
+    };
+    load_chunk(0);
+    store_chunk(0);
+    if (nchunks > 1) load_chunk(1);
+    __syncwarp();
+    int32_t rec = 0, a_prev = 0;
+    const bool band0 = band == 0;
+    for (int blk = 0; blk < nblocks; ++blk) {
+      if (blk > 0) {
+        if (blk < nchunks) store_chunk(blk);
+        __syncwarp();
+        if (blk >= 2 && blk - 2 < nchunks) flush_chunk(blk - 2);
+        if (blk + 1 < nchunks) load_chunk(blk + 1);
+      }
+      const int t0 = blk * 32;
+      const bool edge = t0 < 31 || t0 + 31 >= W;
+      if (edge) enc_block<MED, STEP1, true>(sm, lane, t0, W, maxs, step, half, magic, band0, rec, a_prev);
+      else enc_block<MED, STEP1, false>(sm, lane, t0, W, maxs, step, half, magic, band0, rec, a_prev);
     }
     __syncwarp();
+    for (int j = max(0, nblocks - 2); j < nchunks; ++j) flush_chunk(j);
+    __syncwarp();
   }
+  if (vmax > static_cast<uint32_t>(maxs)) bad = 1;
 }
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
 enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state, int nframes,
                    int64_t total_tiles, ShardInfo* __restrict__ shards, uint32_t* __restrict__ folded,
                    int* __restrict__ queue) {
@@ -247,9 +254,20 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32)
 enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state, int nframes,
                    ShardInfo* __restrict__ shards, int64_t total_shards,
                    const uint32_t* __restrict__ folded, uint8_t* __restrict__ rans_scratch) {
+  // Per warp: one histogram per Rice lane class (symbol i -> class i % 4) and
+  // their total.  For shards whose values are all below 511 -- nearly every
+  // shard -- the 17 Rice sums and the zero-run value cost come from the
+  // histograms over the distinct values; only other shards take a second
+  // per-sample pass.
+  // class rows padded by 8 words: equal values of different classes fall in
+  // different banks
+  __shared__ uint32_t hcls_all[kWarpsPerCta][4][520];
   __shared__ uint32_t hist_all[kWarpsPerCta][512];
+  __shared__ uint16_t list_all[kWarpsPerCta][512];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t (*hcls)[520] = hcls_all[warp];
   uint32_t* hist = hist_all[warp];
+  uint16_t* list = list_all[warp];
   const int64_t warps_total = static_cast<int64_t>(gridDim.x) * kWarpsPerCta;
   for (int64_t s = static_cast<int64_t>(blockIdx.x) * kWarpsPerCta + warp; s < total_shards; s += warps_total) {
     ShardInfo& si = shards[s];
@@ -259,40 +277,36 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     const int n = si.count;
     const uint32_t* __restrict__ f = folded + si.sample_base;
     const int lane_count = min(4, n);
-    for (int i = lane; i < 512; i += 32) hist[i] = 0;
+    for (int i = lane; i < 4 * 520; i += 32) hcls[0][i] = 0;
     __syncwarp();
     uint32_t sk[kMaxRice + 1];
 #pragma unroll
     for (int k = 0; k <= kMaxRice; ++k) sk[k] = 0;
     uint32_t nz_cost = 0;           // per lane: varint bytes of nonzero values
     uint32_t runs = 0, long_runs = 0, cur_run = 0;  // warp-uniform
-    uint32_t block_bytes = 0, bmax = 0, shard_max = 0, zeros = 0;
+    uint32_t block_bytes = 0, bmax = 0, shard_max = 0, zeros = 0, zc = 0;
     const int nchunk = (n + 31) >> 5;
-    for (int m = 0; m < nchunk; ++m) {
+    const uint32_t cls = static_cast<uint32_t>(lane & 3);
+    // pass 1: zero runs, block widths, histograms; four chunks (one 128-symbol
+    // pack block) per iteration, loads issued first
+    for (int m0 = 0; m0 < nchunk; m0 += 4) {
+     uint32_t vv[4];
+#pragma unroll
+     for (int j = 0; j < 4; ++j) {
+       const int idx = (m0 + j) * 32 + lane;
+       vv[j] = idx < n ? __ldg(f + idx) : 0u;
+     }
+#pragma unroll
+     for (int j = 0; j < 4; ++j) {
+      const int m = m0 + j;
+      if (m >= nchunk) break;
       const int idx = m * 32 + lane;
       const bool valid = idx < n;
-      const uint32_t v = valid ? f[idx] : 0u;
-      const uint32_t cmax = __reduce_max_sync(kFull, v);
-      const int kb = bitlen(cmax);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) sk[k] += v >> k;
-      if (kb > 4) {
-#pragma unroll
-        for (int k = 4; k < 8; ++k) sk[k] += v >> k;
-      }
-      if (kb > 8) {
-#pragma unroll
-        for (int k = 8; k < 12; ++k) sk[k] += v >> k;
-      }
-      if (kb > 12) {
-#pragma unroll
-        for (int k = 12; k <= kMaxRice; ++k) sk[k] += v >> k;
-      }
-      // zero-run cost (encode.cu:232-240): value tokens 2v-1, run tokens 2(run-1)
-      nz_cost += v != 0 ? 1u + (v > 64u) + (v > 8192u) + (v > (1u << 20)) : 0u;
+      const uint32_t v = vv[j];
+      zc += valid && v == 0;
+      // zero-run tokens (encode.cu:232-240): runs of zeros cost varint(2(run-1))
       const uint32_t z = __ballot_sync(kFull, valid && v == 0);
       const uint32_t vm = __ballot_sync(kFull, valid);
-      zeros += __popc(z);
       const uint32_t starts = z & ~((z << 1) | (cur_run ? 1u : 0u));
       runs += __popc(starts);
       if (z == vm && vm == kFull) {
@@ -304,8 +318,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
         // trailing zeros up to the last valid symbol start (or extend) the carry
         const int top = 31 - __clz(vm);       // last valid lane
         const uint32_t zz = z << (31 - top);  // align last valid lane to bit 31
-        const uint32_t tail = __clz(~zz);
-        cur_run = tail;
+        cur_run = __clz(~zz);
       }
       // block pack: 4 chunks per 128-symbol block (encode.cu:249-259)
       bmax = max(bmax, v);
@@ -316,7 +329,91 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
         shard_max = max(shard_max, bm);
         bmax = 0;
       }
-      if (valid && v != 0 && v < kRansAlphabet) atomicAdd(&hist[v], 1u);
+      if (valid && v != 0 && v < kRansAlphabet) atomicAdd(&hcls[cls][v], 1u);
+     }
+    }
+    // zeros per class (lanes with equal lane & 3 hold the same class)
+    zc += __shfl_xor_sync(kFull, zc, 4);
+    zc += __shfl_xor_sync(kFull, zc, 8);
+    zc += __shfl_xor_sync(kFull, zc, 16);
+    zeros = __shfl_sync(kFull, zc, 0) + __shfl_sync(kFull, zc, 1) + __shfl_sync(kFull, zc, 2) +
+            __shfl_sync(kFull, zc, 3);
+    if (lane < 4) hcls[lane][0] = zc;
+    __syncwarp();
+    int distinct = 0;
+    uint32_t present = 0;  // bit b: value 16*lane+b present
+    uint32_t cnt_sum = 0;
+    if (shard_max < kRansAlphabet) {
+      // totals and the compact list of present values
+#pragma unroll
+      for (int b = 0; b < 16; ++b) {
+        const int v = lane * 16 + b;
+        const uint32_t h = hcls[0][v] + hcls[1][v] + hcls[2][v] + hcls[3][v];
+        hist[v] = h;
+        present |= (h != 0 ? 1u : 0u) << b;
+        cnt_sum += h;
+      }
+      int rinc = __popc(present);
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int r2 = __shfl_up_sync(kFull, rinc, o);
+        if (lane >= o) rinc += r2;
+      }
+      int r = rinc - __popc(present);
+      for (uint32_t pm = present; pm; pm &= pm - 1) list[r++] = static_cast<uint16_t>(lane * 16 + __ffs(pm) - 1);
+      distinct = __shfl_sync(kFull, rinc, 31);
+      __syncwarp();
+      // Rice sums sum_i (v_i >> k) per class; v < 511 so only k <= 8 count
+      uint32_t S[4][9];
+#pragma unroll
+      for (int l = 0; l < 4; ++l)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) S[l][k] = 0;
+      uint32_t nzc = 0;
+      for (int e = lane; e < distinct; e += 32) {
+        const uint32_t v = list[e];
+        uint32_t tot = 0;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+          const uint32_t c = hcls[l][v];
+          tot += c;
+#pragma unroll
+          for (int k = 0; k < 9; ++k) S[l][k] += c * (v >> k);
+        }
+        // value tokens varint(2v-1): one byte up to v = 64, two below 511
+        nzc += v ? tot * (1u + (v > 64u)) : 0u;
+      }
+      const uint32_t nz_total = warp_sum(nzc);
+      nz_cost = lane == 0 ? nz_total : 0u;
+#pragma unroll
+      for (int l = 0; l < 4; ++l)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          const uint32_t t = warp_sum(S[l][k]);
+          if (lane == l) sk[k] = t;
+        }
+    } else {
+      // pass 2: per-sample Rice sums and value costs
+      for (int m = 0; m < nchunk; ++m) {
+        const int idx = m * 32 + lane;
+        const uint32_t v = idx < n ? __ldg(f + idx) : 0u;
+        const int kb = bitlen(__reduce_max_sync(kFull, v));
+#pragma unroll
+        for (int k = 0; k < 4; ++k) sk[k] += v >> k;
+        if (kb > 4) {
+#pragma unroll
+          for (int k = 4; k < 8; ++k) sk[k] += v >> k;
+        }
+        if (kb > 8) {
+#pragma unroll
+          for (int k = 8; k < 12; ++k) sk[k] += v >> k;
+        }
+        if (kb > 12) {
+#pragma unroll
+          for (int k = 12; k <= kMaxRice; ++k) sk[k] += v >> k;
+        }
+        nz_cost += v != 0 ? 1u + (v > 64u) + (v > 8192u) + (v > (1u << 20)) : 0u;
+      }
     }
     const uint32_t zero_bytes = warp_sum(nz_cost) + runs + long_runs;
     // Rice: reduce the per-lane sums into the four lanes (symbol i -> lane i%4)
@@ -367,19 +464,8 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     // order-0 rANS table (encode.cu:337-392), eligible when max < 511 and
     // at most 255 distinct symbols.
     __syncwarp();
-    if (lane == 0) hist[0] = zeros;
-    __syncwarp();
     int rans_ok = shard_max < kRansAlphabet;
-    uint32_t present = 0;   // bit b: value 16*lane+b present
-    uint32_t cnt_sum = 0;
     if (rans_ok) {
-#pragma unroll
-      for (int b = 0; b < 16; ++b) {
-        const uint32_t h = hist[lane * 16 + b];
-        present |= (h != 0 ? 1u : 0u) << b;
-        cnt_sum += h;
-      }
-      const int distinct = warp_sum(__popc(present));
       if (distinct > 255) rans_ok = 0;
       if (rans_ok) {
         const int D = distinct;
@@ -501,7 +587,8 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
             const int v = lane * 16 + b;
             if (ends[b] >= 0) {
               const uint32_t fr = static_cast<uint32_t>(ends[b] - pe);
-              tab[v] = (fr << 16) | static_cast<uint32_t>(pe);
+              tab[2 * v] = (fr << 16) | static_cast<uint32_t>(pe);
+              tab[2 * v + 1] = fr == 1 ? 0xffffffffu : static_cast<uint32_t>(0x100000000ull / fr);
               uint32_t d = static_cast<uint32_t>(v - pv);
               do {
                 uint8_t byte = d & 0x7f;
@@ -548,6 +635,20 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
 // shards per warp.  Lane bytes are written back to front so they end up in
 // stream order (the reference reverses them at emission, encode.cu:609).
 
+// Division of a rANS state x < 2^31 by a frequency f <= 4096: q' = mulhi(x, m)
+// with m = floor(2^32 / f) (m = 2^32 - 1 for f = 1) is floor(x / f) or one
+// less, since x*m/2^32 > x/f - x/2^32 > x/f - 1; one compare fixes it and
+// yields the remainder as well (reciprocal division with a correction step,
+// Granlund & Montgomery, PLDI 1994).
+__device__ __forceinline__ void div_freq(uint32_t x, uint32_t f, uint32_t m, uint32_t& q, uint32_t& r) {
+  q = __umulhi(x, m);
+  r = x - q * f;
+  if (r >= f) {
+    ++q;
+    r -= f;
+  }
+}
+
 __global__ void __launch_bounds__(128)
 enc_rans_kernel(const FrameState* __restrict__ state, ShardInfo* __restrict__ shards, int64_t total_shards,
                 const uint32_t* __restrict__ folded, uint8_t* __restrict__ rans_scratch) {
@@ -560,28 +661,47 @@ enc_rans_kernel(const FrameState* __restrict__ state, ShardInfo* __restrict__ sh
   const int n = si.count;
   const uint32_t* __restrict__ f = folded + si.sample_base;
   uint8_t* base = rans_scratch + s * static_cast<int64_t>(kRansScratchBytes);
-  const uint32_t* __restrict__ tab = reinterpret_cast<const uint32_t*>(base);
+  const uint2* __restrict__ tab = reinterpret_cast<const uint2*>(base);
   uint32_t* out_end = reinterpret_cast<uint32_t*>(base + kRansTableWords * 4 + kRansSerialBytes +
                                                   (lane + 1) * kRansLaneBytes);
-  uint32_t state_v = kRansL;
-  uint32_t acc = 0;
-  int nbytes = 0;
-  for (int idx = n - 1 - ((n - 1 - lane) & 3); idx >= 0; idx -= 4) {
-    const uint32_t fc = tab[f[idx]];
-    const uint32_t fr = fc >> 16, cum = fc & 0xffffu;
-    const uint32_t thr = fr << 19;  // ((L >> 12) << 8) * freq
-    while (state_v >= thr) {
-      // byte k lands at end-1-k: the first byte of each word is its top byte
-      acc = (acc << 8) | (state_v & 0xffu);
-      ++nbytes;
-      if ((nbytes & 3) == 0) out_end[-(nbytes >> 2)] = acc;
-      state_v >>= 8;
+  uint32_t x = kRansL;
+  uint64_t acc = 0;  // pending bytes, earliest emitted in the highest position
+  int nacc = 0, nwords = 0;
+  const int first = n - 1 - ((n - 1 - lane) & 3);
+  const int steps = first >= 0 ? first / 4 + 1 : 0;  // symbols first, first-4, ..., >= 0
+  constexpr int kAhead = 8;
+  for (int c = 0; c < steps; c += kAhead) {
+    uint32_t v[kAhead];
+    uint2 e[kAhead];
+#pragma unroll
+    for (int j = 0; j < kAhead; ++j) v[j] = (c + j < steps) ? __ldg(f + first - 4 * (c + j)) : 0u;
+#pragma unroll
+    for (int j = 0; j < kAhead; ++j) e[j] = (c + j < steps) ? tab[v[j]] : make_uint2(1u << 16, 0u);
+#pragma unroll
+    for (int j = 0; j < kAhead; ++j) {
+      if (c + j < steps) {
+        const uint32_t fr = e[j].x >> 16, cum = e[j].x & 0xffffu;
+        const uint32_t thr = fr << 19;  // ((L >> 12) << 8) * freq
+        // renormalise: at most two bytes, since x < 2^31 and thr >= 2^19
+        const uint32_t b1 = x >= thr, b2 = (x >> 8) >= thr;
+        const int nb = static_cast<int>(b1 + b2);
+        const uint64_t bytes = b2 ? (((x & 0xffu) << 8) | ((x >> 8) & 0xffu)) : (x & 0xffu);
+        acc = (acc << (8 * nb)) | (nb ? bytes : 0u);
+        nacc += nb;
+        if (nacc >= 4) {
+          nacc -= 4;
+          out_end[-(++nwords)] = static_cast<uint32_t>(acc >> (8 * nacc));
+        }
+        x >>= 8 * nb;
+        uint32_t q, r;
+        div_freq(x, fr, e[j].y, q, r);
+        x = (q << kRansTableLog) + r + cum;
+      }
     }
-    state_v = ((state_v / fr) << kRansTableLog) + state_v % fr + cum;
   }
-  if (nbytes & 3) out_end[-((nbytes >> 2) + 1)] = acc << (8 * (4 - (nbytes & 3)));  // low bytes unused
-  si.rans_lane[lane] = nbytes;
-  si.rans_state[lane] = state_v;
+  if (nacc) out_end[-(nwords + 1)] = static_cast<uint32_t>(acc << (8 * (4 - nacc)));  // low bytes unused
+  si.rans_lane[lane] = 4 * nwords + nacc;
+  si.rans_state[lane] = x;
 }
 
 // ---------------------------------------------------------------------------

@@ -7,8 +7,8 @@
 namespace fvb {
 
 constexpr int kWarpsPerCta = 4;    // warps per CTA of the warp-per-item kernels
-constexpr int kSrcStride = 68;     // u16 ring row stride (64 columns + skew pad)
-constexpr int kFoldStride = 66;    // u32 ring row stride (64 columns + skew pad)
+constexpr int kSrcStride = 66;     // u16 ring row stride: 64 columns + 2 (33 words: conflict-free)
+constexpr int kFoldStride = 65;    // u32 ring row stride: 64 columns + 1 (conflict-free)
 constexpr int kFastMaxW = 512;     // widest tile of the register-wavefront path
 
 // encoder
@@ -29,11 +29,24 @@ __global__ void enc_emit_kernel(const FrameDesc* frames, int nframes, const Shar
 __global__ void enc_prefix_kernel(const FrameDesc* frames, int nframes, const uint8_t* prefix,
                                   uint8_t* const* outs);
 
-// decoder
+// decoder: shards binned by mode (0 rANS, 1 Rice, 2 zero-run, 3 block pack)
+struct DecodeLists {
+  int32_t count[4];
+  int32_t next_group;       // dec_other work counter
+  int32_t next_group_rans;  // dec_rans work counter
+  int32_t pad[2];
+};
+struct RansTable;
 __global__ void dec_parse_kernel(const FrameDesc* frames, FrameState* state, int nframes, int64_t total_tiles,
-                                 ShardInfo* shards);
-__global__ void dec_shards_kernel(const FrameDesc* frames, FrameState* state, const ShardInfo* shards,
-                                  int64_t total_shards, uint32_t* folded);
+                                 ShardInfo* shards, int64_t total_shards, DecodeLists* lists, int32_t* list_items);
+__global__ void dec_rans_tables_kernel(const FrameDesc* frames, FrameState* state, const ShardInfo* shards,
+                                       const DecodeLists* lists, const int32_t* list_items, RansTable* tables);
+__global__ void dec_rans_kernel(const FrameDesc* frames, FrameState* state, const ShardInfo* shards,
+                                DecodeLists* lists, const int32_t* list_items, const RansTable* tables,
+                                uint32_t* folded);
+__global__ void dec_other_kernel(const FrameDesc* frames, FrameState* state, const ShardInfo* shards,
+                                 int64_t total_shards, DecodeLists* lists, const int32_t* list_items,
+                                 uint32_t* folded);
 __global__ void dec_reconstruct_kernel(const FrameDesc* frames, const FrameState* state, int nframes,
                                        int64_t total_tiles, const uint32_t* folded, int* queue);
 __global__ void dec_reconstruct_wide_kernel(const FrameDesc* frames, const FrameState* state, int nframes,
@@ -44,5 +57,7 @@ __global__ void dec_reconstruct_serial_kernel(const FrameDesc* frames, const Fra
 size_t enc_predict_smem();
 size_t enc_emit_smem();
 size_t dec_reconstruct_smem();
+size_t dec_rans_smem();
+size_t dec_rans_table_bytes();
 
 }  // namespace fvb

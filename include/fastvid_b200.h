@@ -136,6 +136,13 @@ int fvb_batch_encode_enqueue(const fvb_frame* frames, int n, void* workspace, in
 int fvb_batch_encode_emit(const fvb_frame* frames, int n, void* workspace, int64_t workspace_bytes,
                           uint8_t* const* outs, void* cuda_stream);
 
+/* Copies the 32-byte header of each device stream into host `headers`
+ * (32 * n bytes) with one gather kernel and one copy, and waits for it.
+ * `scratch` is device memory of at least 16*n rounded up to 256, plus 32*n
+ * bytes. */
+int fvb_gather_headers(const uint8_t* const* streams, const int64_t* stream_lens, int n, void* scratch,
+                       int64_t scratch_bytes, uint8_t* headers, void* cuda_stream);
+
 int fvb_batch_decode_plan(const fvb_frame* frames, int n, int64_t* workspace_bytes);
 
 /* streams[i]/stream_lens[i]: device streams; planes: 3 device pointers per

@@ -943,8 +943,12 @@ static int decode_rans(const uint8_t* body, int64_t body_length, int64_t count,
     const uint32_t value = previous + delta;
     uint32_t fr = (1u << kRansTableLog) - assigned;
     if (i + 1 != n && !read_varint_o0(body, body_length, &cursor, &fr)) return 5;
-    if (fr == 0 || assigned + fr > (1u << kRansTableLog) ||
-        (i + 1 != n && assigned + fr == (1u << kRansTableLog)))
+    /* decode.cu:479-480, with the sum taken without 32-bit wrap-around: a
+     * frequency above 4096 - assigned is rejected even when the reference's
+     * u32 sum would wrap (there the slot-table fill would run past its 4096
+     * entries). */
+    if (fr == 0 || fr > (1u << kRansTableLog) - assigned ||
+        (i + 1 != n && fr == (1u << kRansTableLog) - assigned))
       return 5;
     values[i] = (uint16_t)value;
     freq[i] = (uint16_t)fr;
