@@ -284,7 +284,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     for (int k = 0; k <= kMaxRice; ++k) sk[k] = 0;
     uint32_t nz_cost = 0;           // per lane: varint bytes of nonzero values
     uint32_t runs = 0, long_runs = 0, cur_run = 0;  // warp-uniform
-    uint32_t block_bytes = 0, bmax = 0, shard_max = 0, zeros = 0, zc = 0;
+    uint32_t block_bytes = 0, bmax = 0, shard_max = 0, zc = 0;
     const int nchunk = (n + 31) >> 5;
     const uint32_t cls = static_cast<uint32_t>(lane & 3);
     // pass 1: zero runs, block widths, histograms; four chunks (one 128-symbol
@@ -336,8 +336,6 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     zc += __shfl_xor_sync(kFull, zc, 4);
     zc += __shfl_xor_sync(kFull, zc, 8);
     zc += __shfl_xor_sync(kFull, zc, 16);
-    zeros = __shfl_sync(kFull, zc, 0) + __shfl_sync(kFull, zc, 1) + __shfl_sync(kFull, zc, 2) +
-            __shfl_sync(kFull, zc, 3);
     if (lane < 4) hcls[lane][0] = zc;
     __syncwarp();
     int distinct = 0;
