@@ -55,6 +55,8 @@ SIGNATURES = {
     "fvb_batch_encode_prepare": ([ctypes.POINTER(Frame), c_i32, c_p, c_p, c_p, c_i64, c_p], c_i32),
     "fvb_batch_encode_enqueue": ([ctypes.POINTER(Frame), c_i32, c_p, c_i64, c_p, c_p], c_i32),
     "fvb_batch_encode_emit": ([ctypes.POINTER(Frame), c_i32, c_p, c_i64, c_p, c_p], c_i32),
+    "fvb_decode_noalloc_capacity": ([], c_i64),
+    "fvb_decode_noalloc": ([ctypes.POINTER(Frame), c_p, c_i64, c_p, c_p, c_i32, c_p], c_i32),
     "fvb_gather_headers": ([c_p, c_p, c_i32, c_p, c_i64, c_p, c_p], c_i32),
     "fvb_batch_decode_plan": ([ctypes.POINTER(Frame), c_i32, ctypes.POINTER(c_i64)], c_i32),
     "fvb_batch_decode_prepare": ([ctypes.POINTER(Frame), c_i32, c_p, c_p, c_p, c_p, c_p, c_i64, c_p], c_i32),

@@ -8,6 +8,7 @@
 // analysis pass (encode.cu:806-807) and at the end of decode (decode.cu:718).
 #include <atomic>
 #include <cstdio>
+#include <mutex>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -105,6 +106,9 @@ struct LaunchScope {
 
 constexpr size_t kAlign = 256;
 size_t align_up(size_t v) { return (v + kAlign - 1) & ~(kAlign - 1); }
+
+int fill_decode_descs(const fvb_frame* frames, int n, const uint8_t* const* streams, const int64_t* stream_lens,
+                      uint16_t* const* planes, const int64_t* pitches, FrameDesc* descs);
 
 // quality -> step (encode.cu:71-85)
 int32_t quantization_step(int64_t layout, int64_t depth, int64_t q) {
@@ -718,6 +722,20 @@ int fvb_batch_decode_prepare(const fvb_frame* frames, int n, const uint8_t* cons
   if (rc) return rc;
   cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
   std::vector<FrameDesc> descs(n);
+  rc = fill_decode_descs(frames, n, streams, stream_lens, planes, pitches, descs.data());
+  if (rc) return rc;
+  char* ws = static_cast<char*>(workspace);
+  FVB_CUDA(cudaMemcpyAsync(ws + L.frames, descs.data(), sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, stream));
+  return FVB_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Device descriptors of a decode batch into caller-provided storage.
+int fill_decode_descs(const fvb_frame* frames, int n, const uint8_t* const* streams, const int64_t* stream_lens,
+                      uint16_t* const* planes, const int64_t* pitches, FrameDesc* descs) {
   int64_t tb = 0, sb = 0, nb = 0;
   for (int i = 0; i < n; ++i) {
     FrameDesc& d = descs[i];
@@ -739,10 +757,12 @@ int fvb_batch_decode_prepare(const fvb_frame* frames, int n, const uint8_t* cons
     sb += d.nshards;
     nb += d.nsamples;
   }
-  char* ws = static_cast<char*>(workspace);
-  FVB_CUDA(cudaMemcpyAsync(ws + L.frames, descs.data(), sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, stream));
   return FVB_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void* workspace, int64_t workspace_bytes,
                              int64_t* results, void* cuda_stream) {
@@ -835,6 +855,106 @@ int fvb_decode(const fvb_frame* frame, const uint8_t* stream, int64_t stream_len
   rc = fvb_batch_decode_enqueue(frame, 1, wavefront, workspace, workspace_bytes, res, cuda_stream);
   if (rc) return rc;
   FVB_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(cuda_stream)));
+  if (res[0] != 0) {
+    char buf[96];
+    std::snprintf(buf, sizeof(buf), "malformed entropy payload (CUDA status %lld)", static_cast<long long>(res[0]));
+    return fail(static_cast<int>(res[0]), buf);
+  }
+  return FVB_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Allocation-free decode.
+//
+// Some callers cannot allocate device memory when they decode: plug-ins
+// inside media frameworks that are handed pre-allocated frame buffers while
+// the host application owns the device heap, real-time pipelines that forbid
+// allocation after start-up (cudaMalloc and cudaFree can block and
+// synchronise the device), and components that run under a device-memory
+// budget enforced elsewhere.  fvb_decode_noalloc serves them: its scratch is
+// one file-scope __device__ array of kNoAllocScratchBytes, so the call needs
+// no workspace and allocates nothing.  The array exists on every GPU that
+// loads this library, for the life of the process.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t{32} << 20;  // 32 MiB
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[64] = {nullptr};
+
+// Device address of the scratch array on `device`.  Host code only holds a
+// host-side stand-in for the array's name, so the address is looked up once
+// per device, with that device current, and cached.
+int noalloc_scratch(int device, void** out) {
+  if (device < 0 || device >= 64) return fail(FVB_ERR_ARGUMENT, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_address[device]) {
+    int cur = -1;
+    FVB_CUDA(cudaGetDevice(&cur));
+    if (cur != device) FVB_CUDA(cudaSetDevice(device));
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (cur != device) cudaSetDevice(cur);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_address[device] = ptr;
+  }
+  *out = g_noalloc_address[device];
+  return FVB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t fvb_decode_noalloc_capacity(void) { return static_cast<int64_t>(kNoAllocScratchBytes); }
+
+int fvb_decode_noalloc(const fvb_frame* frame, const uint8_t* stream, int64_t stream_len, uint16_t* const* planes,
+                       const int64_t* pitches, int wavefront, void* cuda_stream) {
+  if (!frame || !stream || !planes || !pitches) return fail(FVB_ERR_ARGUMENT, "null argument");
+  const Totals t = totals_of(frame, 1);
+  const DecLayout L = dec_layout(1, t);
+  if (L.total > kNoAllocScratchBytes) {
+    char buf[192];
+    std::snprintf(buf, sizeof(buf),
+                  "frame needs %zu bytes of decode scratch; the allocation-free decode has %zu "
+                  "(frames up to about 7 million samples)",
+                  L.total, kNoAllocScratchBytes);
+    return fail(FVB_ERR_WORKSPACE, buf);
+  }
+  // the device that holds the output planes does the work
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, planes[0]) != cudaSuccess || attr.type != cudaMemoryTypeDevice) {
+    cudaGetLastError();
+    return fail(FVB_ERR_ARGUMENT, "output planes must be device memory");
+  }
+  void* scratch = nullptr;
+  int rc = noalloc_scratch(attr.device, &scratch);
+  if (rc) return rc;
+  const bool profiling = g_prof.on;  // profiling would create CUDA events
+  g_prof.on = false;
+  uint16_t* p3[3] = {planes[0], frame->planes == 3 ? planes[1] : nullptr, frame->planes == 3 ? planes[2] : nullptr};
+  const int64_t q3[3] = {pitches[0], frame->planes == 3 ? pitches[1] : 0, frame->planes == 3 ? pitches[2] : 0};
+  const uint8_t* s1[1] = {stream};
+  const int64_t l1[1] = {stream_len};
+  cudaStream_t cs = static_cast<cudaStream_t>(cuda_stream);
+  int64_t res[2] = {0, 0};
+  FrameDesc desc;
+  rc = check_ws(scratch, static_cast<int64_t>(kNoAllocScratchBytes), L.total);
+  if (!rc) rc = fill_decode_descs(frame, 1, s1, l1, p3, q3, &desc);
+  if (!rc) {
+    const cudaError_t e = cudaMemcpyAsync(static_cast<char*>(scratch) + L.frames, &desc, sizeof(FrameDesc),
+                                          cudaMemcpyHostToDevice, cs);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(frame descriptor)");
+  }
+  if (!rc) rc = fvb_batch_decode_enqueue(frame, 1, wavefront, scratch, static_cast<int64_t>(kNoAllocScratchBytes),
+                                         res, cuda_stream);
+  g_prof.on = profiling;
+  if (rc) return rc;
+  FVB_CUDA(cudaStreamSynchronize(cs));
   if (res[0] != 0) {
     char buf[96];
     std::snprintf(buf, sizeof(buf), "malformed entropy payload (CUDA status %lld)", static_cast<long long>(res[0]));

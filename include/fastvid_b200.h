@@ -156,6 +156,26 @@ int fvb_batch_decode_prepare(const fvb_frame* frames, int n, const uint8_t* cons
 int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void* workspace,
                              int64_t workspace_bytes, int64_t* results, void* cuda_stream);
 
+/* ---- allocation-free decode (no reference counterpart) --------------------
+ *
+ * For callers that cannot allocate device memory at decode time -- plug-ins
+ * handed pre-allocated frames by a host application that owns the device
+ * heap, real-time pipelines that forbid allocation after start-up (cudaMalloc
+ * and cudaFree can block and synchronise the device), components held to a
+ * device-memory budget enforced elsewhere.  Same contract as fvb_decode, but
+ * the scratch is a fixed 32 MiB array inside the library
+ * (fvb_decode_noalloc_capacity() bytes, frames up to about 7 million samples;
+ * larger frames return FVB_ERR_WORKSPACE), so no workspace is passed and
+ * nothing is allocated.  Every GPU that loads the library holds the array
+ * until the process exits.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  All calls share the one array: calls whose work overlaps
+ * on the GPU (other threads, other streams) race and must be serialised by
+ * the caller; the call itself waits for its result before returning. */
+int64_t fvb_decode_noalloc_capacity(void);
+int fvb_decode_noalloc(const fvb_frame* frame, const uint8_t* stream, int64_t stream_len, uint16_t* const* planes,
+                       const int64_t* pitches, int wavefront, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

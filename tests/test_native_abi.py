@@ -16,7 +16,7 @@ HEADER = Path(__file__).resolve().parent.parent / "include" / "fastvid_b200.h"
 
 def _declared():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(fvb_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(fvb_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol():
