@@ -243,31 +243,42 @@ __global__ void enc_predict_wide_kernel(const FrameDesc* __restrict__ frames, Fr
 }
 
 // ---------------------------------------------------------------------------
-// enc_analyze: one warp per shard.  Lane l of chunk m holds symbol 32m+l, so
-// its Rice lane is l % lane_count for every chunk.
+// enc_analyze: one warp per shard, one 128-symbol pack block per step.  Lane
+// l holds symbols 4l..4l+3 of the block, so component j of every lane is
+// Rice lane j (symbol i -> lane i % 4; shards of fewer than four symbols use
+// lane i as well).
+//
+// Per shard the warp gathers, in one pass over the folded symbols:
+//  * the class histograms (class = Rice lane) -- values below 8, nearly all
+//    symbols of a predicted frame, in per-lane nibble counters, larger values
+//    below 511 with shared-memory atomics;
+//  * the zero-run token count: run starts and runs reaching 65 zeros (whose
+//    varint(2(run-1)) token takes two bytes), from the position of the last
+//    nonzero symbol before each lane (a warp prefix maximum);
+//  * the block-pack widths (encode.cu:249-259) and the shard maximum.
+// The Rice sums sum_i (v_i >> k), the zero-run value bytes and the order-0
+// rANS table then come from the histograms; shards holding a value of 511 or
+// more take a second per-sample pass for the Rice sums instead.
 
 __device__ __forceinline__ int bitlen(uint32_t v) { return 32 - __clz(v); }
-
 __device__ __forceinline__ uint32_t warp_sum(uint32_t v) { return __reduce_add_sync(kFull, v); }
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 8)
 enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state, int nframes,
                    ShardInfo* __restrict__ shards, int64_t total_shards,
                    const uint32_t* __restrict__ folded, uint8_t* __restrict__ rans_scratch) {
-  // Per warp: one histogram per Rice lane class (symbol i -> class i % 4) and
-  // their total.  For shards whose values are all below 511 -- nearly every
-  // shard -- the 17 Rice sums and the zero-run value cost come from the
-  // histograms over the distinct values; only other shards take a second
-  // per-sample pass.
-  // class rows padded by 8 words: equal values of different classes fall in
-  // different banks
-  __shared__ uint32_t hcls_all[kWarpsPerCta][4][520];
-  __shared__ uint32_t hist_all[kWarpsPerCta][512];
-  __shared__ uint16_t list_all[kWarpsPerCta][512];
+  // Class counts: two classes share a 32-bit word (16-bit counts: a class
+  // holds at most 1024 symbols); the words of classes (0,1) and (2,3) of a
+  // value sit 520 words apart, in different banks.  list: the present values
+  // in increasing order, value | total count << 16.
+  __shared__ __align__(16) uint32_t hcls_all[kWarpsPerCta][2][520];
+  __shared__ uint32_t list_all[kWarpsPerCta][512];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t (*hcls)[520] = hcls_all[warp];
-  uint32_t* hist = hist_all[warp];
-  uint16_t* list = list_all[warp];
+  uint32_t* list = list_all[warp];
+  const uint32_t lanes_below = (1u << lane) - 1u;
+  for (int i = lane; i < 2 * 520 / 4; i += 32) reinterpret_cast<uint4*>(hcls[0])[i] = make_uint4(0, 0, 0, 0);
+  __syncwarp();
   const int64_t warps_total = static_cast<int64_t>(gridDim.x) * kWarpsPerCta;
   for (int64_t s = static_cast<int64_t>(blockIdx.x) * kWarpsPerCta + warp; s < total_shards; s += warps_total) {
     ShardInfo& si = shards[s];
@@ -277,121 +288,173 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     const int n = si.count;
     const uint32_t* __restrict__ f = folded + si.sample_base;
     const int lane_count = min(4, n);
-    for (int i = lane; i < 4 * 520; i += 32) hcls[0][i] = 0;
+
+    // ---- pass 1 ----
+    uint32_t nib[4] = {0, 0, 0, 0};    // class j: 4-bit counts of values 0..7
+    uint32_t acc_e[4] = {0, 0, 0, 0};  // class j: 8-bit counts of values 0, 2, 4, 6
+    uint32_t acc_o[4] = {0, 0, 0, 0};  // class j: 8-bit counts of values 1, 3, 5, 7
+    uint32_t runs = 0, long_runs = 0;  // per lane
+    int32_t carry_nz = -1;             // last nonzero position of the blocks so far
+    uint32_t block_bytes = 0, shard_max = 0;  // warp-uniform
+    auto block = [&](const uint32_t (&x)[4], uint32_t valid, int b) {
+      const int p0 = b * kBlockSymbols + 4 * lane;
+      uint32_t zm = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const bool ok = (valid >> j) & 1u;
+        nib[j] += (ok && x[j] < 8u) ? 1u << (4 * x[j]) : 0u;
+        zm |= (ok && x[j] == 0u) ? 1u << j : 0u;
+      }
+      // block pack width (invalid components load as 0)
+      const uint32_t bm = __reduce_max_sync(kFull, max(max(x[0], x[1]), max(x[2], x[3])));
+      shard_max = max(shard_max, bm);
+      block_bytes += 1 + (min(kBlockSymbols, n - b * kBlockSymbols) * bitlen(bm) + 7) / 8;
+      if (bm >= 8u) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (((valid >> j) & 1u) && x[j] >= 8u && x[j] < static_cast<uint32_t>(kRansAlphabet))
+            atomicAdd(&hcls[j >> 1][x[j]], 1u << (16 * (j & 1)));
+      }
+      // zero runs; positions past the shard end count as nonzero
+      const uint32_t nzm = ~zm & 0xfu;
+      int32_t last = nzm ? p0 + 31 - __clz(nzm) : -1;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) last = max(last, __shfl_up_sync(kFull, last, o));
+      const int32_t up = __shfl_up_sync(kFull, last, 1);
+      const int32_t before = lane ? max(up, carry_nz) : carry_nz;  // last nonzero before p0
+      carry_nz = max(carry_nz, __shfl_sync(kFull, last, 31));
+      // a zero starts a run when its predecessor is nonzero (or the shard start)
+      runs += __popc(zm & ((nzm << 1) | (before == p0 - 1 ? 1u : 0u)));
+      // the run through p0 has p0-1-before zeros ahead of it; it reaches 65
+      // zeros at component 64-(p0-1-before) if the zeros last that far
+      const uint32_t jh = static_cast<uint32_t>(64 - (p0 - 1 - before));
+      if (jh < 4u) {
+        const uint32_t need = (2u << jh) - 1u;
+        long_runs += (zm & need) == need;
+      }
+      if ((b & 7) == 7) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc_e[j] += nib[j] & 0x0f0f0f0fu;
+          acc_o[j] += (nib[j] >> 4) & 0x0f0f0f0fu;
+          nib[j] = 0;
+        }
+      }
+    };
+    const int nblk = (n + kBlockSymbols - 1) / kBlockSymbols;
+    const bool aligned = (reinterpret_cast<uintptr_t>(f) & 15u) == 0;
+    const int nfull = aligned ? n / kBlockSymbols : 0;
+    {
+      // whole blocks: one 16-byte load per lane, two blocks in flight
+      const uint4* __restrict__ f4 = reinterpret_cast<const uint4*>(f);
+      uint4 qa = make_uint4(0, 0, 0, 0), qb = make_uint4(0, 0, 0, 0);
+      if (nfull > 0) qa = __ldg(f4 + lane);
+      if (nfull > 1) qb = __ldg(f4 + 32 + lane);
+      for (int b = 0; b < nfull; ++b) {
+        const uint32_t x[4] = {qa.x, qa.y, qa.z, qa.w};
+        qa = qb;
+        if (b + 2 < nfull) qb = __ldg(f4 + (b + 2) * 32 + lane);
+        block(x, 0xfu, b);
+      }
+    }
+    for (int b = nfull; b < nblk; ++b) {
+      // the ragged last block, or every block of an unaligned shard
+      const int p0 = b * kBlockSymbols + 4 * lane;
+      uint32_t x[4];
+      uint32_t valid = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const bool ok = p0 + j < n;
+        x[j] = ok ? __ldg(f + p0 + j) : 0u;
+        valid |= ok ? 1u << j : 0u;
+      }
+      block(x, valid, b);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      acc_e[j] += nib[j] & 0x0f0f0f0fu;
+      acc_o[j] += (nib[j] >> 4) & 0x0f0f0f0fu;
+    }
+    // warp totals of the small-value counts, as class-pair words; their
+    // Rice sums for k = 0..2 (values below 8 have v >> 3 == 0)
+    uint32_t small01[3] = {0, 0, 0}, small23[3] = {0, 0, 0};
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      const int sh = 8 * (v >> 1);
+      const uint32_t c0 = (((v & 1) ? acc_o[0] : acc_e[0]) >> sh) & 0xffu;
+      const uint32_t c1 = (((v & 1) ? acc_o[1] : acc_e[1]) >> sh) & 0xffu;
+      const uint32_t c2 = (((v & 1) ? acc_o[2] : acc_e[2]) >> sh) & 0xffu;
+      const uint32_t c3 = (((v & 1) ? acc_o[3] : acc_e[3]) >> sh) & 0xffu;
+      const uint32_t w01 = warp_sum(c0 | (c1 << 16));
+      const uint32_t w23 = warp_sum(c2 | (c3 << 16));
+      if (lane == v) {
+        hcls[0][v] = w01;
+        hcls[1][v] = w23;
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        small01[k] += w01 * static_cast<uint32_t>(v >> k);
+        small23[k] += w23 * static_cast<uint32_t>(v >> k);
+      }
+    }
     __syncwarp();
+    const uint32_t zero_runs = warp_sum(runs) + warp_sum(long_runs);
+
     uint32_t sk[kMaxRice + 1];
 #pragma unroll
     for (int k = 0; k <= kMaxRice; ++k) sk[k] = 0;
-    uint32_t nz_cost = 0;           // per lane: varint bytes of nonzero values
-    uint32_t runs = 0, long_runs = 0, cur_run = 0;  // warp-uniform
-    uint32_t block_bytes = 0, bmax = 0, shard_max = 0, zc = 0;
-    const int nchunk = (n + 31) >> 5;
-    const uint32_t cls = static_cast<uint32_t>(lane & 3);
-    // pass 1: zero runs, block widths, histograms; four chunks (one 128-symbol
-    // pack block) per iteration, loads issued first
-    for (int m0 = 0; m0 < nchunk; m0 += 4) {
-     uint32_t vv[4];
-#pragma unroll
-     for (int j = 0; j < 4; ++j) {
-       const int idx = (m0 + j) * 32 + lane;
-       vv[j] = idx < n ? __ldg(f + idx) : 0u;
-     }
-#pragma unroll
-     for (int j = 0; j < 4; ++j) {
-      const int m = m0 + j;
-      if (m >= nchunk) break;
-      const int idx = m * 32 + lane;
-      const bool valid = idx < n;
-      const uint32_t v = vv[j];
-      zc += valid && v == 0;
-      // zero-run tokens (encode.cu:232-240): runs of zeros cost varint(2(run-1))
-      const uint32_t z = __ballot_sync(kFull, valid && v == 0);
-      const uint32_t vm = __ballot_sync(kFull, valid);
-      const uint32_t starts = z & ~((z << 1) | (cur_run ? 1u : 0u));
-      runs += __popc(starts);
-      if (z == vm && vm == kFull) {
-        if (cur_run <= 64 && cur_run + 32 > 64) ++long_runs;
-        cur_run += 32;
-      } else {
-        const uint32_t lead = __ffs(~z) - 1;  // zeros continuing the carried run
-        if (cur_run <= 64 && cur_run + lead > 64) ++long_runs;
-        // trailing zeros up to the last valid symbol start (or extend) the carry
-        const int top = 31 - __clz(vm);       // last valid lane
-        const uint32_t zz = z << (31 - top);  // align last valid lane to bit 31
-        cur_run = __clz(~zz);
-      }
-      // block pack: 4 chunks per 128-symbol block (encode.cu:249-259)
-      bmax = max(bmax, v);
-      if ((m & 3) == 3 || m == nchunk - 1) {
-        const uint32_t bm = __reduce_max_sync(kFull, bmax);
-        const int nb = min(kBlockSymbols, n - (m & ~3) * 32);
-        block_bytes += 1 + (nb * bitlen(bm) + 7) / 8;
-        shard_max = max(shard_max, bm);
-        bmax = 0;
-      }
-      if (valid && v != 0 && v < kRansAlphabet) atomicAdd(&hcls[cls][v], 1u);
-     }
-    }
-    // zeros per class (lanes with equal lane & 3 hold the same class)
-    zc += __shfl_xor_sync(kFull, zc, 4);
-    zc += __shfl_xor_sync(kFull, zc, 8);
-    zc += __shfl_xor_sync(kFull, zc, 16);
-    if (lane < 4) hcls[lane][0] = zc;
-    __syncwarp();
+    uint32_t nz_cost = 0;  // varint bytes of the nonzero value tokens
     int distinct = 0;
-    uint32_t present = 0;  // bit b: value 16*lane+b present
-    uint32_t cnt_sum = 0;
-    if (shard_max < kRansAlphabet) {
-      // totals and the compact list of present values
-#pragma unroll
-      for (int b = 0; b < 16; ++b) {
-        const int v = lane * 16 + b;
-        const uint32_t h = hcls[0][v] + hcls[1][v] + hcls[2][v] + hcls[3][v];
-        hist[v] = h;
-        present |= (h != 0 ? 1u : 0u) << b;
-        cnt_sum += h;
-      }
-      int rinc = __popc(present);
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int r2 = __shfl_up_sync(kFull, rinc, o);
-        if (lane >= o) rinc += r2;
-      }
-      int r = rinc - __popc(present);
-      for (uint32_t pm = present; pm; pm &= pm - 1) list[r++] = static_cast<uint16_t>(lane * 16 + __ffs(pm) - 1);
-      distinct = __shfl_sync(kFull, rinc, 31);
-      __syncwarp();
-      // Rice sums sum_i (v_i >> k) per class; v < 511 so only k <= 8 count
-      uint32_t S[4][9];
-#pragma unroll
-      for (int l = 0; l < 4; ++l)
-#pragma unroll
-        for (int k = 0; k < 9; ++k) S[l][k] = 0;
+    if (shard_max < static_cast<uint32_t>(kRansAlphabet)) {
+      // the list of present values and the value-token bytes: varint(2v-1)
+      // is one byte up to v = 64 and two below 511
+      int small_present = 0;
       uint32_t nzc = 0;
-      for (int e = lane; e < distinct; e += 32) {
-        const uint32_t v = list[e];
-        uint32_t tot = 0;
-#pragma unroll
-        for (int l = 0; l < 4; ++l) {
-          const uint32_t c = hcls[l][v];
-          tot += c;
-#pragma unroll
-          for (int k = 0; k < 9; ++k) S[l][k] += c * (v >> k);
-        }
-        // value tokens varint(2v-1): one byte up to v = 64, two below 511
-        nzc += v ? tot * (1u + (v > 64u)) : 0u;
+      const int iters = static_cast<int>(shard_max >> 5) + 1;
+      for (int it = 0; it < iters; ++it) {
+        const int v = it * 32 + lane;
+        const uint32_t w01 = hcls[0][v], w23 = hcls[1][v];
+        const uint32_t h = (w01 & 0xffffu) + (w01 >> 16) + (w23 & 0xffffu) + (w23 >> 16);
+        const uint32_t pres = __ballot_sync(kFull, h != 0);
+        if (h) list[distinct + __popc(pres & lanes_below)] = static_cast<uint32_t>(v) | (h << 16);
+        if (it == 0) small_present = __popc(pres & 0xffu);
+        distinct += __popc(pres);
+        nzc += v ? h * (1u + (v > 64)) : 0u;
       }
-      const uint32_t nz_total = warp_sum(nzc);
-      nz_cost = lane == 0 ? nz_total : 0u;
+      nz_cost = warp_sum(nzc);
+      __syncwarp();
+      // Rice sums, class l in lane l: the small values' part plus, one class
+      // at a time, the values from 8 up
+      const int cl = lane & 3;
+      const uint32_t sel = lane < 4 ? 0xffffffffu : 0u;
 #pragma unroll
-      for (int l = 0; l < 4; ++l)
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t w = (cl >> 1) ? small23[k] : small01[k];
+        sk[k] = ((w >> (16 * (cl & 1))) & 0xffffu) & sel;
+      }
+      if (distinct > small_present) {
+#pragma unroll 1
+        for (int l = 0; l < 4; ++l) {
+          uint32_t S[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          const uint32_t t = warp_sum(S[l][k]);
-          if (lane == l) sk[k] = t;
+          for (int k = 0; k < 9; ++k) S[k] = 0;
+          for (int e = small_present + lane; e < distinct; e += 32) {
+            const uint32_t v = list[e] & 0xffffu;
+            const uint32_t c = (hcls[l >> 1][v] >> (16 * (l & 1))) & 0xffffu;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) S[k] += c * (v >> k);
+          }
+#pragma unroll
+          for (int k = 0; k < 9; ++k) {
+            const uint32_t t = warp_sum(S[k]);
+            if (lane == l) sk[k] += t;
+          }
         }
+      }
     } else {
-      // pass 2: per-sample Rice sums and value costs
+      // pass 2: per-sample Rice sums and value costs, lane i % 32 of each
+      // 32-symbol chunk (Rice lane i % 4 = lane % 4)
+      const int nchunk = (n + 31) >> 5;
       for (int m = 0; m < nchunk; ++m) {
         const int idx = m * 32 + lane;
         const uint32_t v = idx < n ? __ldg(f + idx) : 0u;
@@ -412,9 +475,19 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
         }
         nz_cost += v != 0 ? 1u + (v > 64u) + (v > 8192u) + (v > (1u << 20)) : 0u;
       }
+      nz_cost = warp_sum(nz_cost);
+#pragma unroll
+      for (int k = 0; k <= kMaxRice; ++k) {
+        uint32_t v = sk[k];
+        v += __shfl_xor_sync(kFull, v, 4);
+        v += __shfl_xor_sync(kFull, v, 8);
+        v += __shfl_xor_sync(kFull, v, 16);
+        sk[k] = lane < 4 ? v : 0u;
+      }
     }
-    const uint32_t zero_bytes = warp_sum(nz_cost) + runs + long_runs;
-    // Rice: reduce the per-lane sums into the four lanes (symbol i -> lane i%4)
+    const uint32_t zero_bytes = nz_cost + zero_runs;
+
+    // Rice: lane l < lane_count holds the sums of Rice lane l
     int64_t best_bytes = INT64_MAX;
     int best_k = 0;
     uint32_t lane_bytes_best = 0;
@@ -422,10 +495,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     const int nsym = rl < lane_count ? (n - rl + lane_count - 1) / lane_count : 0;
 #pragma unroll
     for (int k = 0; k <= kMaxRice; ++k) {
-      uint32_t v = sk[k];
-      v += __shfl_xor_sync(kFull, v, 4);
-      v += __shfl_xor_sync(kFull, v, 8);
-      v += __shfl_xor_sync(kFull, v, 16);
+      const uint32_t v = __shfl_sync(kFull, sk[k], rl);
       const uint32_t bits = v + static_cast<uint32_t>(nsym) * (1u + k);
       const uint32_t lb = rl < lane_count ? (bits + 7) / 8 : 0u;
       uint32_t tot = lb + __shfl_xor_sync(kFull, lb, 1);
@@ -460,170 +530,113 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     if (lane < 4) si.comp_lane[lane] = lane < lane_count ? static_cast<int32_t>(lane_bytes_best) : 0;
 
     // order-0 rANS table (encode.cu:337-392), eligible when max < 511 and
-    // at most 255 distinct symbols.
-    __syncwarp();
-    int rans_ok = shard_max < kRansAlphabet;
+    // at most 255 distinct symbols; one list entry per lane.
+    const int rans_ok = shard_max < static_cast<uint32_t>(kRansAlphabet) && distinct <= 255;
     if (rans_ok) {
-      if (distinct > 255) rans_ok = 0;
-      if (rans_ok) {
-        const int D = distinct;
-        // exclusive prefix of counts and ranks over lanes
-        uint32_t cinc = cnt_sum, rinc = __popc(present);
+      // Normalisation as a prefix maximum: for the i-th present symbol,
+      // end_i = i + min(max(1, max_{j<=i}(f_j - j)), 4097 - D) with
+      // f_j = floor(P_j * 4096 / n), P_j the count of symbols up to the j-th;
+      // the last symbol ends at 4096.  This equals the reference's clamp loop
+      // (encode.cu:370-390): writing u_i = end_i - i turns
+      // end_i = min(max(f_i, end_{i-1}+1), 4097-D+i) into
+      // u_i = min(max(f_i - i, u_{i-1}), 4097-D) with u_{-1} = 1.
+      const int D = distinct;
+      const int32_t G = 4097 - D;
+      // floor(x / n) for x <= 2^24 by a multiply-high with floor((2^32-1)/n)
+      // and one correction (the estimate is exact or one low)
+      const uint32_t un = static_cast<uint32_t>(n);
+      const uint32_t ninv = 0xffffffffu / un;
+      uint32_t* tab = reinterpret_cast<uint32_t*>(rans_scratch + s * static_cast<int64_t>(kRansScratchBytes));
+      uint8_t* ser = rans_scratch + s * static_cast<int64_t>(kRansScratchBytes) + kRansTableWords * 4;
+      const int head = 1 + varint_len(static_cast<uint32_t>(D));
+      uint32_t c_count = 0, c_cursor = static_cast<uint32_t>(head);
+      int32_t c_u = 1, c_end = 0, c_v = 0;
+      for (int e0 = 0; e0 < D; e0 += 32) {
+        const int e = e0 + lane;
+        const bool ok = e < D;
+        const uint32_t ent = ok ? list[e] : 0u;
+        const int32_t v = static_cast<int32_t>(ent & 0xffffu);
+        uint32_t P = ent >> 16;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t c2 = __shfl_up_sync(kFull, cinc, o), r2 = __shfl_up_sync(kFull, rinc, o);
-          if (lane >= o) {
-            cinc += c2;
-            rinc += r2;
-          }
+          const uint32_t t = __shfl_up_sync(kFull, P, o);
+          if (lane >= o) P += t;
         }
-        uint32_t P = cinc - cnt_sum;
-        int rank = static_cast<int>(rinc) - __popc(present);
-        // normalisation as a prefix maximum: for the i-th present symbol,
-        // end_i = i + min(max(1, max_{j<=i}(f_j - j)), 4097 - D) with
-        // f_j = floor(P_j * 4096 / n); the last symbol ends at 4096.  This
-        // equals the reference's clamp loop (encode.cu:370-390): writing
-        // u_i = end_i - i turns end_i = min(max(f_i, end_{i-1}+1), 4097-D+i)
-        // into u_i = min(max(f_i - i, u_{i-1}), 4097-D) with u_{-1} = 1.
-        int32_t dmax = INT32_MIN;
-        {
-          uint32_t p = P;
-          int r = rank;
+        P += c_count;
+        const uint32_t x = P << kRansTableLog;
+        uint32_t q = __umulhi(x, ninv);
+        if (x - q * un >= un) ++q;
+        int32_t u = ok ? static_cast<int32_t>(q) - e : INT32_MIN;
 #pragma unroll
-          for (int b = 0; b < 16; ++b) {
-            const uint32_t h = hist[lane * 16 + b];
-            if (h) {
-              p += h;
-              const int32_t fj = static_cast<int32_t>((p << kRansTableLog) / static_cast<uint32_t>(n));
-              dmax = max(dmax, fj - r);
-              ++r;
-            }
-          }
+        for (int o = 1; o < 32; o <<= 1) u = max(u, __shfl_up_sync(kFull, u, o));
+        u = max(u, c_u);
+        const int32_t end = e == D - 1 ? (1 << kRansTableLog) : e + min(u, G);
+        int32_t pe = __shfl_up_sync(kFull, end, 1), pv = __shfl_up_sync(kFull, v, 1);
+        if (lane == 0) {
+          pe = c_end;
+          pv = c_v;
         }
-        int32_t dinc = dmax;
+        const uint32_t fr = static_cast<uint32_t>(end - pe);
+        const uint32_t dv = static_cast<uint32_t>(v - pv);
+        const uint32_t bytes = ok ? varint_len(dv) + (e != D - 1 ? varint_len(fr) : 0) : 0u;
+        uint32_t binc = bytes;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-          const int32_t d2 = __shfl_up_sync(kFull, dinc, o);
-          if (lane >= o) dinc = max(dinc, d2);
+          const uint32_t t = __shfl_up_sync(kFull, binc, o);
+          if (lane >= o) binc += t;
         }
-        int32_t dpre = __shfl_up_sync(kFull, dinc, 1);
-        if (lane == 0) dpre = INT32_MIN;
-        // ends, cumulative starts and serialised table lengths
-        uint32_t* tab = reinterpret_cast<uint32_t*>(rans_scratch + s * static_cast<int64_t>(kRansScratchBytes));
-        const int G = 4097 - D;
-        int32_t ends[16];
-        int32_t run_max = dpre;
-        uint32_t p = P;
-        int r = rank;
-        int32_t last_end_lane = 0;
-#pragma unroll
-        for (int b = 0; b < 16; ++b) {
-          const uint32_t h = hist[lane * 16 + b];
-          ends[b] = -1;
-          if (h) {
-            p += h;
-            const int32_t fj = static_cast<int32_t>((p << kRansTableLog) / static_cast<uint32_t>(n));
-            run_max = max(run_max, fj - r);
-            ends[b] = (r == D - 1) ? (1 << kRansTableLog) : r + min(max(1, run_max), G);
-            last_end_lane = ends[b];
-            ++r;
-          }
-        }
-        // previous end (cumulative) = exclusive prefix max of ends
-        int32_t einc = last_end_lane;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int32_t e2 = __shfl_up_sync(kFull, einc, o);
-          if (lane >= o) einc = max(einc, e2);
-        }
-        int32_t prev_end = __shfl_up_sync(kFull, einc, 1);
-        if (lane == 0) prev_end = 0;
-        // previous present value (for table deltas): exclusive prefix max
-        int32_t last_v = -1;
-#pragma unroll
-        for (int b = 0; b < 16; ++b)
-          if (ends[b] >= 0) last_v = lane * 16 + b;
-        int32_t vinc = last_v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int32_t v2 = __shfl_up_sync(kFull, vinc, o);
-          if (lane >= o) vinc = max(vinc, v2);
-        }
-        int32_t prev_v = __shfl_up_sync(kFull, vinc, 1);
-        if (lane == 0 || prev_v < 0) prev_v = 0;
-        // per-lane byte count of the serialised entries
-        uint32_t my_bytes = 0;
-        {
-          int32_t pe = prev_end, pv = prev_v;
-          int rr = rank;
-#pragma unroll
-          for (int b = 0; b < 16; ++b) {
-            if (ends[b] >= 0) {
-              const int v = lane * 16 + b;
-              my_bytes += varint_len(static_cast<uint32_t>(v - pv));
-              if (rr != D - 1) my_bytes += varint_len(static_cast<uint32_t>(ends[b] - pe));
-              pe = ends[b];
-              pv = v;
-              ++rr;
-            }
-          }
-        }
-        uint32_t binc = my_bytes;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t b2 = __shfl_up_sync(kFull, binc, o);
-          if (lane >= o) binc += b2;
-        }
-        const int head = 1 + varint_len(static_cast<uint32_t>(D));
-        uint8_t* ser = rans_scratch + s * static_cast<int64_t>(kRansScratchBytes) + kRansTableWords * 4;
-        uint32_t cursor = head + binc - my_bytes;
-        {
-          int32_t pe = prev_end, pv = prev_v;
-          int rr = rank;
-#pragma unroll
-          for (int b = 0; b < 16; ++b) {
-            const int v = lane * 16 + b;
-            if (ends[b] >= 0) {
-              const uint32_t fr = static_cast<uint32_t>(ends[b] - pe);
-              tab[2 * v] = (fr << 16) | static_cast<uint32_t>(pe);
-              tab[2 * v + 1] = fr == 1 ? 0xffffffffu : static_cast<uint32_t>(0x100000000ull / fr);
-              uint32_t d = static_cast<uint32_t>(v - pv);
-              do {
-                uint8_t byte = d & 0x7f;
-                d >>= 7;
-                if (d) byte |= 0x80;
-                ser[cursor++] = byte;
-              } while (d);
-              if (rr != D - 1) {
-                uint32_t e = fr;
-                do {
-                  uint8_t byte = e & 0x7f;
-                  e >>= 7;
-                  if (e) byte |= 0x80;
-                  ser[cursor++] = byte;
-                } while (e);
-              }
-              pe = ends[b];
-              pv = v;
-              ++rr;
-            }
-          }
-        }
-        if (lane == 31) {
-          ser[0] = kRansTableLog;
-          uint32_t d = static_cast<uint32_t>(D);
-          int c = 1;
+        if (ok) {
+          // floor(2^32 / fr): floor((2^32-1) / fr), plus one when fr is a
+          // power of two; 2^32 - 1 for fr = 1
+          const uint32_t recip =
+              fr == 1 ? 0xffffffffu : 0xffffffffu / fr + ((fr & (fr - 1)) == 0 ? 1u : 0u);
+          tab[2 * v] = (fr << 16) | static_cast<uint32_t>(pe);
+          tab[2 * v + 1] = recip;
+          uint32_t cursor = c_cursor + binc - bytes;
+          uint32_t d = dv;
           do {
             uint8_t byte = d & 0x7f;
             d >>= 7;
             if (d) byte |= 0x80;
-            ser[c++] = byte;
+            ser[cursor++] = byte;
           } while (d);
-          si.rans_table = head + static_cast<int32_t>(binc);
+          if (e != D - 1) {
+            uint32_t w = fr;
+            do {
+              uint8_t byte = w & 0x7f;
+              w >>= 7;
+              if (w) byte |= 0x80;
+              ser[cursor++] = byte;
+            } while (w);
+          }
         }
+        c_count = __shfl_sync(kFull, P, 31);
+        c_u = __shfl_sync(kFull, u, 31);
+        c_end = __shfl_sync(kFull, end, 31);
+        c_v = __shfl_sync(kFull, v, 31);
+        c_cursor += __shfl_sync(kFull, binc, 31);
+      }
+      if (lane == 0) {
+        ser[0] = kRansTableLog;
+        uint32_t d = static_cast<uint32_t>(D);
+        int c = 1;
+        do {
+          uint8_t byte = d & 0x7f;
+          d >>= 7;
+          if (d) byte |= 0x80;
+          ser[c++] = byte;
+        } while (d);
+        si.rans_table = static_cast<int32_t>(c_cursor);
       }
     }
     if (lane == 0) si.rans_ok = rans_ok;
+    // clear the histogram bins this shard used
+    __syncwarp();
+    const int used = static_cast<int>(min(shard_max, static_cast<uint32_t>(kRansAlphabet - 1)) >> 5) + 1;
+    for (int it = 0; it < used; ++it) {
+      hcls[0][it * 32 + lane] = 0;
+      hcls[1][it * 32 + lane] = 0;
+    }
     __syncwarp();
   }
 }
