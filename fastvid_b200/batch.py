@@ -65,7 +65,10 @@ class BatchCodec:
     """
 
     def __init__(self, device=None, use_graphs: bool = True, max_cached_shapes: int = 8):
-        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        dev = torch.device(device) if device is not None else torch.device("cuda")
+        if dev.type != "cuda":
+            raise RuntimeError("BatchCodec needs a CUDA device")
+        self.device = dev if dev.index is not None else torch.device("cuda", torch.cuda.current_device())
         self.use_graphs = use_graphs
         self.max_cached = max_cached_shapes
         self._enc: dict = {}

@@ -258,10 +258,25 @@ int ensure_smem_attrs() {
 // ---------------------------------------------------------------------------
 // workspace layouts
 
+// Encoder passes a frame may need: gray10 frames with a step above 1 may
+// re-run with the MED predictor, gray16 frames with a step above 1 may refine
+// their step twice (encode.cu frame policy; the device decides whether a
+// later pass actually runs).
+int frame_passes(const fvb_frame& f) {
+  if (f.layout == 0 && f.bit_depth == 10 && f.step > 1) return 2;
+  if (f.layout == 0 && f.bit_depth == 16 && f.step > 1) return 3;
+  return 1;
+}
+constexpr int kMaxPasses = 3;
+
 struct Totals {
   int64_t tiles = 0, shards = 0, samples = 0, prefix = 0;
   bool wide = false;
   int passes = 1;
+  // frames, tiles and shards that take part in pass p; the encoder lays the
+  // batch out with frames of more passes first, so these are prefixes
+  int frames_p[kMaxPasses] = {0, 0, 0};
+  int64_t tiles_p[kMaxPasses] = {0, 0, 0}, shards_p[kMaxPasses] = {0, 0, 0};
 };
 
 Totals totals_of(const fvb_frame* frames, int n) {
@@ -274,12 +289,26 @@ Totals totals_of(const fvb_frame* frames, int n) {
     t.prefix += f.prefix_bytes;
     const int64_t ptw0 = f.tile_w;
     if (ptw0 > kFastMaxW) t.wide = true;
-    int passes = 1;
-    if (f.layout == 0 && f.bit_depth == 10 && f.step > 1) passes = 2;
-    if (f.layout == 0 && f.bit_depth == 16 && f.step > 1) passes = 3;
+    const int passes = frame_passes(f);
     if (passes > t.passes) t.passes = passes;
+    for (int p = 0; p < passes; ++p) {
+      ++t.frames_p[p];
+      t.tiles_p[p] += f.tiles;
+      t.shards_p[p] += f.shards;
+    }
   }
   return t;
+}
+
+// Encoder batch layout order: frames needing three passes, then two, then
+// one, each group in the caller's order.
+std::vector<int> encode_order(const fvb_frame* frames, int n) {
+  std::vector<int> order;
+  order.reserve(n);
+  for (int passes = kMaxPasses; passes >= 1; --passes)
+    for (int i = 0; i < n; ++i)
+      if (frame_passes(frames[i]) == passes) order.push_back(i);
+  return order;
 }
 
 struct EncLayout {
@@ -341,11 +370,13 @@ __global__ void gather_headers_kernel(const uint8_t* const* __restrict__ streams
   out[i] = b < lens[k] ? streams[k][b] : 0;
 }
 
-__global__ void results_kernel(const FrameState* __restrict__ state, int n, int64_t* __restrict__ out, int decode) {
+__global__ void results_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state, int n,
+                               int64_t* __restrict__ out, int decode) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  out[2 * i] = state[i].status;
-  out[2 * i + 1] = decode ? 0 : state[i].stream_len;
+  const int slot = frames[i].slot;
+  out[2 * slot] = state[i].status;
+  out[2 * slot + 1] = decode ? 0 : state[i].stream_len;
 }
 
 int check_ws(void* ws, int64_t ws_bytes, size_t need) {
@@ -474,10 +505,13 @@ int fvb_batch_encode_prepare(const fvb_frame* frames, int n, const uint16_t* con
   if (rc) return rc;
   cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
   std::vector<FrameDesc> descs(n);
+  const std::vector<int> order = encode_order(frames, n);
   int64_t tb = 0, sb = 0, nb = 0, pb = 0;
-  for (int i = 0; i < n; ++i) {
-    FrameDesc& d = descs[i];
+  for (int j = 0; j < n; ++j) {
+    const int i = order[j];
+    FrameDesc& d = descs[j];
     build_desc(frames[i], d, frames[i].layout != 0);
+    d.slot = i;
     for (int p = 0; p < d.planes; ++p) {
       const uint16_t* ptr = planes[3 * i + p];
       if (!ptr) return fail(FVB_ERR_ARGUMENT, "null plane pointer");
@@ -523,44 +557,47 @@ int fvb_batch_encode_enqueue(const fvb_frame* frames, int n, void* workspace, in
     enc_init_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, n);
   }
   FVB_LAUNCHED("enc_init_kernel");
-  const int g_pred = grid_for(t.tiles, kWarpsPerCta, 4);
-  const int g_an = grid_for(t.shards, kWarpsPerCta, 16);
-  const int g_rans = static_cast<int>(ceil_div(t.shards * 4 > 0 ? t.shards * 4 : 1, 128));
+  // pass p covers the batch's first frames_p[p] frames (layout order)
   for (int pass = 0; pass < t.passes; ++pass) {
+    const int nf = t.frames_p[pass];
+    const int64_t tiles = t.tiles_p[pass], nsh = t.shards_p[pass];
     FVB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), stream));
     {
       LaunchScope scope_(K_ENC_PREDICT, stream);
-      enc_predict_kernel<<<g_pred, kWarpsPerCta * 32, enc_predict_smem(), stream>>>(frames_d, state, n, t.tiles, shards,
-                                                                                   folded, queue);
+      enc_predict_kernel<<<grid_for(tiles, kWarpsPerCta, 4), kWarpsPerCta * 32, enc_predict_smem(), stream>>>(
+          frames_d, state, nf, tiles, shards, folded, queue);
     }
     FVB_LAUNCHED("enc_predict_kernel");
     if (t.wide) {
       {
         LaunchScope scope_(K_ENC_PREDICT_WIDE, stream);
-        enc_predict_wide_kernel<<<grid_for(t.tiles, 1, 8), 256, 0, stream>>>(frames_d, state, n, t.tiles, folded, recon);
+        enc_predict_wide_kernel<<<grid_for(tiles, 1, 8), 256, 0, stream>>>(frames_d, state, nf, tiles, folded, recon);
       }
       FVB_LAUNCHED("enc_predict_wide_kernel");
     }
     {
+      // resident CTAs only: each warp streams its shards through one ring
       LaunchScope scope_(K_ENC_ANALYZE, stream);
-      enc_analyze_kernel<<<g_an, kWarpsPerCta * 32, 0, stream>>>(frames_d, state, n, shards, t.shards, folded, rans);
+      enc_analyze_kernel<<<grid_for(nsh, kWarpsPerCta, 6), kWarpsPerCta * 32, 0, stream>>>(frames_d, state, nf, shards,
+                                                                                           nsh, folded, rans);
     }
     FVB_LAUNCHED("enc_analyze_kernel");
     {
       LaunchScope scope_(K_ENC_RANS, stream);
-      enc_rans_kernel<<<g_rans, 128, 0, stream>>>(state, shards, t.shards, folded, rans);
+      enc_rans_kernel<<<static_cast<int>(ceil_div(nsh * 4 > 0 ? nsh * 4 : 1, 128)), 128, 0, stream>>>(
+          state, shards, nsh, folded, rans);
     }
     FVB_LAUNCHED("enc_rans_kernel");
     {
       LaunchScope scope_(K_ENC_SCAN, stream);
-      enc_scan_kernel<<<n, 1024, 0, stream>>>(frames_d, state, n, shards, prefix);
+      enc_scan_kernel<<<nf, 1024, 0, stream>>>(frames_d, state, nf, shards, prefix);
     }
     FVB_LAUNCHED("enc_scan_kernel");
   }
   int64_t* res_d = reinterpret_cast<int64_t*>(ws + L.results);
   {
     LaunchScope scope_(K_RESULTS, stream);
-    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(state, n, res_d, 0);
+    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, n, res_d, 0);
   }
   FVB_LAUNCHED("results_kernel");
   if (results) FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
@@ -581,7 +618,10 @@ int fvb_batch_encode_emit(const fvb_frame* frames, int n, void* workspace, int64
   cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
   char* ws = static_cast<char*>(workspace);
   uint8_t** outs_d = reinterpret_cast<uint8_t**>(ws + L.outs);
-  FVB_CUDA(cudaMemcpyAsync(outs_d, outs, sizeof(uint8_t*) * n, cudaMemcpyHostToDevice, stream));
+  std::vector<uint8_t*> outs_laid(n);  // in batch layout order
+  const std::vector<int> order = encode_order(frames, n);
+  for (int j = 0; j < n; ++j) outs_laid[j] = outs[order[j]];
+  FVB_CUDA(cudaMemcpyAsync(outs_d, outs_laid.data(), sizeof(uint8_t*) * n, cudaMemcpyHostToDevice, stream));
   const FrameDesc* frames_d = reinterpret_cast<const FrameDesc*>(ws + L.frames);
   int64_t max_prefix = 0;
   for (int i = 0; i < n; ++i) max_prefix = frames[i].prefix_bytes > max_prefix ? frames[i].prefix_bytes : max_prefix;
@@ -741,6 +781,7 @@ int fill_decode_descs(const fvb_frame* frames, int n, const uint8_t* const* stre
     FrameDesc& d = descs[i];
     const bool gray = frames[i].layout == 0;
     build_desc(frames[i], d, ((frames[i].flags & 0x40) != 0) || !gray);
+    d.slot = i;
     if (!streams[i]) return fail(FVB_ERR_ARGUMENT, "null stream pointer");
     d.stream = streams[i];
     d.stream_len = stream_lens[i];
@@ -835,7 +876,7 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
   int64_t* res_d = reinterpret_cast<int64_t*>(ws + L.results);
   {
     LaunchScope scope_(K_RESULTS, stream);
-    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(state, n, res_d, 1);
+    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, n, res_d, 1);
   }
   FVB_LAUNCHED("results_kernel");
   if (results) FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));

@@ -71,6 +71,8 @@ struct FrameDesc {
   int64_t tile_base, shard_base, sample_base;  // placement in the batch arrays
   int64_t prefix_base;   // byte offset of this frame's header+directory in prefix scratch
   int64_t prefix_bytes;  // 32 + 32 * ntiles
+  int32_t slot;          // the frame's index in the caller's batch (results, outputs)
+  int32_t pad_slot;
   // I/O
   const uint16_t* src[3];
   int64_t src_pitch[3];  // elements
@@ -159,6 +161,22 @@ __device__ inline int find_frame(const int64_t* bases, int n, int64_t idx) {
 }
 
 __device__ inline void set_status(int32_t* status, int32_t code) { atomicCAS(status, 0, code); }
+
+// Asynchronous global -> shared copies (cp.async, sm_80+), completed per
+// thread with commit/wait groups.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 __device__ __forceinline__ int varint_len(uint32_t v) {
   return v < (1u << 7) ? 1 : v < (1u << 14) ? 2 : v < (1u << 21) ? 3 : v < (1u << 28) ? 4 : 5;

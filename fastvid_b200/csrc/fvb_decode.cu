@@ -226,14 +226,6 @@ struct ByteWindow {
   }
 };
 
-// Asynchronous 4-byte global -> shared copies (cp.async, sm_80+).
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait2() { asm volatile("cp.async.wait_group 2;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // A lane's byte stream through a private 16-word ring in shared memory, fed
 // by cp.async four words at a time and kept 12-15 words ahead of the read
@@ -272,7 +264,7 @@ struct LaneRing {
   __device__ void read2(int cur, uint32_t& b0, uint32_t& b1) {
     const int pos = head + cur;
     if (fetched - (pos >> 2) < 12) fetch4();
-    cp_async_wait2();  // the two newest groups may stay in flight
+    cp_async_wait<2>();  // the two newest groups may stay in flight
     const uint8_t* rb = reinterpret_cast<const uint8_t*>(ring);
     b0 = rb[pos & 63];
     b1 = rb[(pos + 1) & 63];
@@ -485,7 +477,7 @@ dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
         cur += nb;
         ring.read2(cur, b0, b1);
       }
-      cp_async_wait0();
+      cp_async_wait<0>();
       if (cur != llen || x != kRansL) set_status(&state[si.frame].status, 5);
     }
     __syncwarp();

@@ -248,114 +248,203 @@ __global__ void enc_predict_wide_kernel(const FrameDesc* __restrict__ frames, Fr
 // Rice lane j (symbol i -> lane i % 4; shards of fewer than four symbols use
 // lane i as well).
 //
-// Per shard the warp gathers, in one pass over the folded symbols:
+// Pass 1 gathers per shard:
 //  * the class histograms (class = Rice lane) -- values below 8, nearly all
 //    symbols of a predicted frame, in per-lane nibble counters, larger values
 //    below 511 with shared-memory atomics;
-//  * the zero-run token count: run starts and runs reaching 65 zeros (whose
-//    varint(2(run-1)) token takes two bytes), from the position of the last
-//    nonzero symbol before each lane (a warp prefix maximum);
 //  * the block-pack widths (encode.cu:249-259) and the shard maximum.
 // The Rice sums sum_i (v_i >> k), the zero-run value bytes and the order-0
 // rANS table then come from the histograms; shards holding a value of 511 or
-// more take a second per-sample pass for the Rice sums instead.
+// more take a second per-sample pass for the Rice sums instead.  The
+// zero-run run tokens are counted (in one more pass) only for shards whose
+// value tokens alone do not already lose to block packing or Rice coding.
 
 __device__ __forceinline__ int bitlen(uint32_t v) { return 32 - __clz(v); }
 __device__ __forceinline__ uint32_t warp_sum(uint32_t v) { return __reduce_add_sync(kFull, v); }
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32, 8)
+// 1 << s for s < 32 and 0 for larger s (PTX shl clamps the shift amount)
+__device__ __forceinline__ uint32_t bit_or_zero(uint32_t s) {
+  uint32_t r;
+  asm("shl.b32 %0, %1, %2;" : "=r"(r) : "r"(1u), "r"(s));
+  return r;
+}
+
+// Zero-run token statistics of one 128-symbol block (encode.cu:232-240): a
+// run of zeros costs varint(2(run-1)), one byte up to 64 zeros and two beyond
+// (a shard holds at most 4096 symbols).  zm: this lane's zero components at
+// positions p0..p0+3; positions past the shard end count as nonzero.
+struct RunStats {
+  int32_t carry = -1;      // last nonzero position of the blocks so far
+  uint32_t runs = 0;       // runs started (per lane)
+  uint32_t long_runs = 0;  // runs that reached 65 zeros (per lane)
+};
+
+__device__ __forceinline__ void run_block(RunStats& r, uint32_t zm, int32_t p0, int lane) {
+  const uint32_t nzm = ~zm & 0xfu;
+  int32_t last = nzm ? p0 + 31 - __clz(nzm) : -1;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) last = max(last, __shfl_up_sync(kFull, last, o));
+  const int32_t up = __shfl_up_sync(kFull, last, 1);
+  const int32_t before = lane ? max(up, r.carry) : r.carry;  // last nonzero before p0
+  r.carry = max(r.carry, __shfl_sync(kFull, last, 31));
+  // a zero starts a run when its predecessor is nonzero (or the shard start)
+  r.runs += __popc(zm & ((nzm << 1) | (before == p0 - 1 ? 1u : 0u)));
+  // the run through p0 has p0-1-before zeros ahead of it; it reaches 65
+  // zeros at component 64-(p0-1-before) if the zeros last that far
+  const uint32_t jh = static_cast<uint32_t>(64 - (p0 - 1 - before));
+  if (jh < 4u) {
+    const uint32_t need = (2u << jh) - 1u;
+    r.long_runs += (zm & need) == need;
+  }
+}
+
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 6)
 enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state, int nframes,
                    ShardInfo* __restrict__ shards, int64_t total_shards,
                    const uint32_t* __restrict__ folded, uint8_t* __restrict__ rans_scratch) {
   // Class counts: two classes share a 32-bit word (16-bit counts: a class
   // holds at most 1024 symbols); the words of classes (0,1) and (2,3) of a
   // value sit 520 words apart, in different banks.  list: the present values
-  // in increasing order, value | total count << 16.
+  // in increasing order, value | total count << 16.  ring: each lane's next
+  // kRing 16-byte pieces of the warp's block stream.
+  constexpr int kRing = 6;
   __shared__ __align__(16) uint32_t hcls_all[kWarpsPerCta][2][520];
   __shared__ uint32_t list_all[kWarpsPerCta][512];
+  __shared__ __align__(16) uint4 ring_all[kWarpsPerCta][kRing * 32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t (*hcls)[520] = hcls_all[warp];
   uint32_t* list = list_all[warp];
+  uint4* ring = ring_all[warp];
   const uint32_t lanes_below = (1u << lane) - 1u;
   for (int i = lane; i < 2 * 520 / 4; i += 32) reinterpret_cast<uint4*>(hcls[0])[i] = make_uint4(0, 0, 0, 0);
   __syncwarp();
+  // frames of this pass (bit per frame, the first kMaskFrames frames; later
+  // frames are treated as active until their own flag is read)
+  constexpr int kMaskFrames = 4096;
+  __shared__ uint32_t active_mask[kMaskFrames / 32];
+  const int mask_words = min((nframes + 31) / 32, kMaskFrames / 32);
+  for (int w = warp; w < mask_words; w += kWarpsPerCta) {
+    const int i = w * 32 + lane;
+    const uint32_t m = __ballot_sync(kFull, i < nframes && state[i].active);
+    if (lane == 0) active_mask[w] = m;
+  }
+  __syncthreads();
+  auto streamed = [&](int32_t frame) {
+    return frame >= kMaskFrames || ((active_mask[frame >> 5] >> (frame & 31)) & 1u);
+  };
   const int64_t warps_total = static_cast<int64_t>(gridDim.x) * kWarpsPerCta;
-  for (int64_t s = static_cast<int64_t>(blockIdx.x) * kWarpsPerCta + warp; s < total_shards; s += warps_total) {
+  const int64_t s0 = static_cast<int64_t>(blockIdx.x) * kWarpsPerCta + warp;
+  // Whole blocks of a shard that starts 16-byte aligned are read through the
+  // ring; the ragged last block and unaligned shards use direct loads.
+  // Shards of frames that sit this pass out are skipped by both sides.
+  auto whole_blocks = [&](int32_t count, int64_t base, int32_t frame) {
+    return streamed(frame) && (reinterpret_cast<uintptr_t>(folded + base) & 15u) == 0 ? count / kBlockSymbols : 0;
+  };
+  // Producer: the warp's whole blocks in shard order, kRing pieces ahead of
+  // the consumer and across shard boundaries, one commit group per piece
+  // (empty past the end), so piece i sits in slot i % kRing and its group is
+  // complete once at most kRing - 1 newer groups are pending.
+  int64_t pt = s0;      // shard being fetched
+  int pc = 0, pnf = 0;  // next block and whole blocks of pt
+  const uint4* pp = nullptr;
+  int32_t q_count = 0, q_frame = 0;  // shard pt + warps_total, loaded one shard early
+  int64_t q_base = 0;
+  int pslot = 0;
+  if (pt < total_shards) {
+    pnf = whole_blocks(shards[pt].count, shards[pt].sample_base, shards[pt].frame);
+    pp = reinterpret_cast<const uint4*>(folded + shards[pt].sample_base);
+    if (pt + warps_total < total_shards) {
+      q_count = shards[pt + warps_total].count;
+      q_frame = shards[pt + warps_total].frame;
+      q_base = shards[pt + warps_total].sample_base;
+    }
+  }
+  auto issue = [&]() {
+    while (pc >= pnf && pt < total_shards) {
+      pt += warps_total;
+      pc = 0;
+      if (pt < total_shards) {
+        pnf = whole_blocks(q_count, q_base, q_frame);
+        pp = reinterpret_cast<const uint4*>(folded + q_base);
+        if (pt + warps_total < total_shards) {
+          q_count = shards[pt + warps_total].count;
+          q_frame = shards[pt + warps_total].frame;
+          q_base = shards[pt + warps_total].sample_base;
+        }
+      }
+    }
+    if (pt < total_shards) {
+      cp_async16(ring + pslot * 32 + lane, pp + pc * 32 + lane);
+      ++pc;
+    }
+    cp_async_commit();
+    pslot = pslot + 1 == kRing ? 0 : pslot + 1;
+  };
+  for (int i = 0; i < kRing; ++i) issue();
+  int cslot = 0;
+  // consumer: the next shard's descriptor is loaded while this one runs
+  int32_t h_count = 0, h_frame = 0;
+  int64_t h_base = 0;
+  if (s0 < total_shards) {
+    h_count = shards[s0].count;
+    h_frame = shards[s0].frame;
+    h_base = shards[s0].sample_base;
+  }
+  for (int64_t s = s0; s < total_shards; s += warps_total) {
     ShardInfo& si = shards[s];
-    const int fi = si.frame;
-    FrameState& st = state[fi];
-    if (!st.active) continue;
-    const int n = si.count;
-    const uint32_t* __restrict__ f = folded + si.sample_base;
+    const int n = h_count;
+    const int64_t base = h_base;
+    const int32_t frame = h_frame;
+    if (s + warps_total < total_shards) {
+      h_count = shards[s + warps_total].count;
+      h_frame = shards[s + warps_total].frame;
+      h_base = shards[s + warps_total].sample_base;
+    }
+    if (!streamed(frame)) continue;
+    FrameState& st = state[frame];
+    const int32_t active = st.active;  // first needed after pass 1
+    const uint32_t* __restrict__ f = folded + base;
     const int lane_count = min(4, n);
 
     // ---- pass 1 ----
     uint32_t nib[4] = {0, 0, 0, 0};    // class j: 4-bit counts of values 0..7
     uint32_t acc_e[4] = {0, 0, 0, 0};  // class j: 8-bit counts of values 0, 2, 4, 6
     uint32_t acc_o[4] = {0, 0, 0, 0};  // class j: 8-bit counts of values 1, 3, 5, 7
-    uint32_t runs = 0, long_runs = 0;  // per lane
-    int32_t carry_nz = -1;             // last nonzero position of the blocks so far
-    uint32_t block_bytes = 0, shard_max = 0;  // warp-uniform
-    auto block = [&](const uint32_t (&x)[4], uint32_t valid, int b) {
-      const int p0 = b * kBlockSymbols + 4 * lane;
-      uint32_t zm = 0;
+    uint32_t shard_max = 0, clz_sum = 0, tail_bytes = 0;  // warp-uniform
+    auto flush = [&]() {
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const bool ok = (valid >> j) & 1u;
-        nib[j] += (ok && x[j] < 8u) ? 1u << (4 * x[j]) : 0u;
-        zm |= (ok && x[j] == 0u) ? 1u << j : 0u;
-      }
-      // block pack width (invalid components load as 0)
-      const uint32_t bm = __reduce_max_sync(kFull, max(max(x[0], x[1]), max(x[2], x[3])));
-      shard_max = max(shard_max, bm);
-      block_bytes += 1 + (min(kBlockSymbols, n - b * kBlockSymbols) * bitlen(bm) + 7) / 8;
-      if (bm >= 8u) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (((valid >> j) & 1u) && x[j] >= 8u && x[j] < static_cast<uint32_t>(kRansAlphabet))
-            atomicAdd(&hcls[j >> 1][x[j]], 1u << (16 * (j & 1)));
-      }
-      // zero runs; positions past the shard end count as nonzero
-      const uint32_t nzm = ~zm & 0xfu;
-      int32_t last = nzm ? p0 + 31 - __clz(nzm) : -1;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) last = max(last, __shfl_up_sync(kFull, last, o));
-      const int32_t up = __shfl_up_sync(kFull, last, 1);
-      const int32_t before = lane ? max(up, carry_nz) : carry_nz;  // last nonzero before p0
-      carry_nz = max(carry_nz, __shfl_sync(kFull, last, 31));
-      // a zero starts a run when its predecessor is nonzero (or the shard start)
-      runs += __popc(zm & ((nzm << 1) | (before == p0 - 1 ? 1u : 0u)));
-      // the run through p0 has p0-1-before zeros ahead of it; it reaches 65
-      // zeros at component 64-(p0-1-before) if the zeros last that far
-      const uint32_t jh = static_cast<uint32_t>(64 - (p0 - 1 - before));
-      if (jh < 4u) {
-        const uint32_t need = (2u << jh) - 1u;
-        long_runs += (zm & need) == need;
-      }
-      if ((b & 7) == 7) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          acc_e[j] += nib[j] & 0x0f0f0f0fu;
-          acc_o[j] += (nib[j] >> 4) & 0x0f0f0f0fu;
-          nib[j] = 0;
-        }
+        acc_e[j] += nib[j] & 0x0f0f0f0fu;
+        acc_o[j] += (nib[j] >> 4) & 0x0f0f0f0fu;
+        nib[j] = 0;
       }
     };
+    auto count_big = [&](const uint32_t (&x)[4], uint32_t valid) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (((valid >> j) & 1u) && x[j] >= 8u && x[j] < static_cast<uint32_t>(kRansAlphabet))
+          atomicAdd(&hcls[j >> 1][x[j]], 1u << (16 * (j & 1)));
+    };
     const int nblk = (n + kBlockSymbols - 1) / kBlockSymbols;
-    const bool aligned = (reinterpret_cast<uintptr_t>(f) & 15u) == 0;
-    const int nfull = aligned ? n / kBlockSymbols : 0;
-    {
-      // whole blocks: one 16-byte load per lane, two blocks in flight
-      const uint4* __restrict__ f4 = reinterpret_cast<const uint4*>(f);
-      uint4 qa = make_uint4(0, 0, 0, 0), qb = make_uint4(0, 0, 0, 0);
-      if (nfull > 0) qa = __ldg(f4 + lane);
-      if (nfull > 1) qb = __ldg(f4 + 32 + lane);
-      for (int b = 0; b < nfull; ++b) {
-        const uint32_t x[4] = {qa.x, qa.y, qa.z, qa.w};
-        qa = qb;
-        if (b + 2 < nfull) qb = __ldg(f4 + (b + 2) * 32 + lane);
-        block(x, 0xfu, b);
+    const int nfull = whole_blocks(n, base, frame);
+    // whole blocks from the ring; the nibble counters take at most 8 blocks
+    // between flushes
+    for (int g = 0; g < nfull; g += 8) {
+      const int ge = min(g + 8, nfull);
+      for (int b = g; b < ge; ++b) {
+        cp_async_wait<kRing - 1>();
+        const uint4 q = ring[cslot * 32 + lane];
+        const uint32_t x[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) nib[j] += bit_or_zero(x[j] << 2);  // values >= 8 add nothing
+        const uint32_t bm = __reduce_max_sync(kFull, max(max(x[0], x[1]), max(x[2], x[3])));
+        issue();  // refills the slot just read
+        cslot = cslot + 1 == kRing ? 0 : cslot + 1;
+        shard_max = max(shard_max, bm);
+        clz_sum += __clz(bm);  // block bytes 1 + 128 * bitlen / 8
+        if (bm >= 8u) count_big(x, 0xfu);
       }
+      flush();
     }
     for (int b = nfull; b < nblk; ++b) {
       // the ragged last block, or every block of an unaligned shard
@@ -367,26 +456,41 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
         const bool ok = p0 + j < n;
         x[j] = ok ? __ldg(f + p0 + j) : 0u;
         valid |= ok ? 1u << j : 0u;
+        nib[j] += ok ? bit_or_zero(x[j] << 2) : 0u;
       }
-      block(x, valid, b);
+      const uint32_t bm = __reduce_max_sync(kFull, max(max(x[0], x[1]), max(x[2], x[3])));
+      shard_max = max(shard_max, bm);
+      tail_bytes += 1 + (min(kBlockSymbols, n - b * kBlockSymbols) * bitlen(bm) + 7) / 8;
+      if (bm >= 8u) count_big(x, valid);
+      if ((b & 7) == 7) flush();
     }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      acc_e[j] += nib[j] & 0x0f0f0f0fu;
-      acc_o[j] += (nib[j] >> 4) & 0x0f0f0f0fu;
+    flush();
+    const uint32_t block_bytes = static_cast<uint32_t>(nfull) * 513u - 16u * clz_sum + tail_bytes;
+    // clear the histogram bins the atomics of this shard may have touched
+    auto clear_bins = [&]() {
+      __syncwarp();
+      const int used = static_cast<int>(min(shard_max, static_cast<uint32_t>(kRansAlphabet - 1)) >> 5) + 1;
+      for (int it = 0; it < used; ++it) {
+        hcls[0][it * 32 + lane] = 0;
+        hcls[1][it * 32 + lane] = 0;
+      }
+      __syncwarp();
+    };
+    if (!active) {  // a frame past the active mask that sits this pass out: nothing written
+      clear_bins();
+      continue;
     }
     // warp totals of the small-value counts, as class-pair words; their
     // Rice sums for k = 0..2 (values below 8 have v >> 3 == 0)
     uint32_t small01[3] = {0, 0, 0}, small23[3] = {0, 0, 0};
 #pragma unroll
     for (int v = 0; v < 8; ++v) {
-      const int sh = 8 * (v >> 1);
-      const uint32_t c0 = (((v & 1) ? acc_o[0] : acc_e[0]) >> sh) & 0xffu;
-      const uint32_t c1 = (((v & 1) ? acc_o[1] : acc_e[1]) >> sh) & 0xffu;
-      const uint32_t c2 = (((v & 1) ? acc_o[2] : acc_e[2]) >> sh) & 0xffu;
-      const uint32_t c3 = (((v & 1) ? acc_o[3] : acc_e[3]) >> sh) & 0xffu;
-      const uint32_t w01 = warp_sum(c0 | (c1 << 16));
-      const uint32_t w23 = warp_sum(c2 | (c3 << 16));
+      // byte v/2 of classes (0,1) resp. (2,3) into the two 16-bit halves
+      const uint32_t sel = static_cast<uint32_t>(v >> 1) | ((4u + static_cast<uint32_t>(v >> 1)) << 8);
+      const uint32_t w01 =
+          warp_sum(__byte_perm((v & 1) ? acc_o[0] : acc_e[0], (v & 1) ? acc_o[1] : acc_e[1], sel) & 0x00ff00ffu);
+      const uint32_t w23 =
+          warp_sum(__byte_perm((v & 1) ? acc_o[2] : acc_e[2], (v & 1) ? acc_o[3] : acc_e[3], sel) & 0x00ff00ffu);
       if (lane == v) {
         hcls[0][v] = w01;
         hcls[1][v] = w23;
@@ -398,7 +502,6 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
       }
     }
     __syncwarp();
-    const uint32_t zero_runs = warp_sum(runs) + warp_sum(long_runs);
 
     uint32_t sk[kMaxRice + 1];
 #pragma unroll
@@ -485,16 +588,17 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
         sk[k] = lane < 4 ? v : 0u;
       }
     }
-    const uint32_t zero_bytes = nz_cost + zero_runs;
-
     // Rice: lane l < lane_count holds the sums of Rice lane l
     int64_t best_bytes = INT64_MAX;
     int best_k = 0;
     uint32_t lane_bytes_best = 0;
     const int rl = lane & 3;
     const int nsym = rl < lane_count ? (n - rl + lane_count - 1) / lane_count : 0;
+    // sums vanish beyond the shard's bit length, where the cost only grows
+    const int kstop = min(kMaxRice, bitlen(shard_max));
 #pragma unroll
     for (int k = 0; k <= kMaxRice; ++k) {
+      if (k > kstop) break;
       const uint32_t v = __shfl_sync(kFull, sk[k], rl);
       const uint32_t bits = v + static_cast<uint32_t>(nsym) * (1u + k);
       const uint32_t lb = rl < lane_count ? (bits + 7) / 8 : 0u;
@@ -507,12 +611,27 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
       }
     }
     const int64_t rice_body = static_cast<int64_t>(lane_count - 1) * 4 + best_bytes;
+    // zero-run coding wins only if its bytes are at most both others'; the
+    // value tokens alone bound them from below
+    int64_t zero_bytes = INT64_MAX;
+    if (static_cast<int64_t>(nz_cost) <= min(static_cast<int64_t>(block_bytes), rice_body)) {
+      RunStats rs;
+      for (int b = 0; b < nblk; ++b) {
+        const int p0 = b * kBlockSymbols + 4 * lane;
+        uint32_t zm = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (p0 + j < n && __ldg(f + p0 + j) == 0u) zm |= 1u << j;
+        run_block(rs, zm, p0, lane);
+      }
+      zero_bytes = static_cast<int64_t>(nz_cost) + warp_sum(rs.runs) + warp_sum(rs.long_runs);
+    }
     int mode;
     int64_t body;
     if (static_cast<int64_t>(block_bytes) < zero_bytes && static_cast<int64_t>(block_bytes) < rice_body) {
       mode = kModeBlockPack;
       body = block_bytes;
-    } else if (static_cast<int64_t>(zero_bytes) <= rice_body) {
+    } else if (zero_bytes <= rice_body) {
       mode = kModeZeroRun;
       body = zero_bytes;
     } else {
@@ -630,15 +749,9 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
       }
     }
     if (lane == 0) si.rans_ok = rans_ok;
-    // clear the histogram bins this shard used
-    __syncwarp();
-    const int used = static_cast<int>(min(shard_max, static_cast<uint32_t>(kRansAlphabet - 1)) >> 5) + 1;
-    for (int it = 0; it < used; ++it) {
-      hcls[0][it * 32 + lane] = 0;
-      hcls[1][it * 32 + lane] = 0;
-    }
-    __syncwarp();
+    clear_bins();
   }
+  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
