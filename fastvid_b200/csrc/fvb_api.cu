@@ -841,7 +841,8 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
   FVB_LAUNCHED("dec_rans_tables_kernel");
   {
     LaunchScope scope_(K_DEC_RANS, stream);
-    dec_rans_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), 1, 12), 32, dec_rans_smem(), stream>>>(
+    dec_rans_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), kWarpsPerCta, 16), kWarpsPerCta * 32, dec_rans_smem(),
+                      stream>>>(
         frames_d, state, shards, lists, items, tables, folded);
   }
   FVB_LAUNCHED("dec_rans_kernel");

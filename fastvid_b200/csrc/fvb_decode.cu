@@ -146,8 +146,12 @@ __global__ void dec_parse_kernel(const FrameDesc* __restrict__ frames, FrameStat
 //                    zero-run shard g on lane 4g (decode.cu:237-295), block
 //                    shards one after another warp-wide (decode.cu:342-396)
 
+// Measured on the 48-frame mix: 32-slot buckets, 16-word rings and a 3 KB
+// pool beat 8- and 16-slot buckets, 8-word rings and a one-ahead symbol
+// lookup (1.51 ms against 1.51-1.68 ms).
 constexpr int kGroup = 8;        // shards per warp
-constexpr int kCoarseShift = 3;  // coarse bucket = 8 slots
+constexpr int kCoarseShift = 5;  // coarse bucket = 32 slots
+constexpr int kRingWords = 16;   // words of a lane's byte ring
 
 struct RansTable {
   int32_t lane_start[4], lane_len[4];
@@ -227,27 +231,29 @@ struct ByteWindow {
 };
 
 
-// A lane's byte stream through a private 16-word ring in shared memory, fed
-// by cp.async four words at a time and kept 12-15 words ahead of the read
-// position: reads are shared-memory loads whose data arrived long before.
-// Word w of the aligned range lives in ring slot w & 15; only words holding a
-// byte of the lane are copied (others keep stale bytes, and reading them is
-// an overrun that the byte count check reports).
+// A lane's byte stream through a private ring of kRingWords words in shared
+// memory, fed by cp.async kRingWords/4 words at a time and kept at least
+// 3/4 of the ring ahead of the read position: reads are shared-memory loads
+// whose data arrived long before.  Word w of the aligned range lives in slot
+// w % kRingWords; only words holding a byte of the lane are copied (others
+// keep stale bytes, and reading them is an overrun that the byte count check
+// reports).
 struct LaneRing {
-  uint32_t* ring;          // 16 words of shared memory
+  static constexpr int kStep = kRingWords / 4;  // words per commit group
+  uint32_t* ring;          // kRingWords words of shared memory
   const uint32_t* words;   // aligned base of the lane's bytes
   int head;                // lane byte 0 = byte `head` of word 0
   int last;                // last word holding a lane byte (-1: none)
-  int fetched;             // words issued so far (multiple of 4)
+  int fetched;             // words issued so far
 
-  __device__ void fetch4() {
+  __device__ void fetch() {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < kStep; ++j) {
       const int w = fetched + j;
-      if (w <= last) cp_async4(ring + (w & 15), words + w);
+      if (w <= last) cp_async4(ring + (w & (kRingWords - 1)), words + w);
     }
     cp_async_commit();
-    fetched += 4;
+    fetched += kStep;
   }
   __device__ void init(uint32_t* ring_smem, const uint8_t* p, int len) {
     const uintptr_t a = reinterpret_cast<uintptr_t>(p);
@@ -256,18 +262,21 @@ struct LaneRing {
     ring = ring_smem;
     last = len > 0 ? (head + len - 1) >> 2 : -1;
     fetched = 0;
-    fetch4();
-    fetch4();
-    fetch4();
+    fetch();
+    fetch();
+    fetch();
   }
-  // make the bytes at lane positions cur, cur+1 readable and return them
-  __device__ void read2(int cur, uint32_t& b0, uint32_t& b1) {
+  // The four bytes at lane positions cur..cur+3, first byte in the top bits;
+  // cur advances by at most four between calls.  After a fetch the ring
+  // holds words w .. w + 3/4 ring - 1 or more; all but the newest group are
+  // complete, which covers words w and w + 1.
+  __device__ uint32_t window(int cur) {
     const int pos = head + cur;
-    if (fetched - (pos >> 2) < 12) fetch4();
-    cp_async_wait<2>();  // the two newest groups may stay in flight
-    const uint8_t* rb = reinterpret_cast<const uint8_t*>(ring);
-    b0 = rb[pos & 63];
-    b1 = rb[(pos + 1) & 63];
+    const int w = pos >> 2;
+    if (fetched - w < 3 * kStep) fetch();
+    cp_async_wait<1>();  // the newest group may stay in flight
+    const uint32_t lo = ring[w & (kRingWords - 1)], hi = ring[(w + 1) & (kRingWords - 1)];
+    return __byte_perm(__funnelshift_r(lo, hi, 8 * (pos & 3)), 0, 0x0123);
   }
 };
 
@@ -371,28 +380,36 @@ dec_rans_tables_kernel(const FrameDesc* __restrict__ frames, FrameState* __restr
   }
 }
 
-struct RansShardSm {
-  uint8_t coarse[(1 << kRansTableLog) >> kCoarseShift];  // first symbol of each 8-slot bucket
-  uint2 info[256];
+// Shared memory of one dec_rans warp.  A round's tables sit back to back in
+// `pool`: per shard a coarse table (first symbol of each 32-slot bucket,
+// 128 bytes) followed by its nsym info entries -- a few hundred bytes for the
+// handful of symbols a predicted shard holds, so many warps fit on an SM.  A group of eight shards whose tables exceed the pool is decoded in
+// several rounds.
+constexpr int kRansPoolUnits = 384;  // uint2 units: 3 KB
+constexpr int kCoarseBuckets = (1 << kRansTableLog) >> kCoarseShift;
+constexpr int kCoarseUnits = kCoarseBuckets / 8;
+
+struct RansWarpSm {
+  uint2 pool[kRansPoolUnits];
+  // per-lane byte rings; a row one word longer than the ring puts equal
+  // ring slots of different lanes in different banks.  While tables are
+  // built (no decode in flight) the first 128 words hold the symbol-start
+  // bitmap.
+  uint32_t rings[32][kRingWords + 1];
+  int32_t off[kGroup];  // pool offset of each shard of the round (-1: not decoded)
 };
+static_assert(32 * (kRingWords + 1) >= 128, "bitmap alias");
 
-struct RansGroupSm {
-  RansShardSm r[kGroup];
-  uint32_t bitmap[128];
-  uint32_t rings[32][16];  // per-lane byte-stream rings
-  int32_t valid[kGroup];
-};
+size_t dec_rans_smem() { return sizeof(RansWarpSm) * kWarpsPerCta; }
 
-size_t dec_rans_smem() { return sizeof(RansGroupSm); }
-
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(kWarpsPerCta * 32)
 dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
                 const ShardInfo* __restrict__ shards, DecodeLists* __restrict__ lists,
                 const int32_t* __restrict__ list_items, const RansTable* __restrict__ tables,
                 uint32_t* __restrict__ folded) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  RansGroupSm& sm = *reinterpret_cast<RansGroupSm*>(smem_raw);
-  const int lane = threadIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  RansWarpSm& sm = reinterpret_cast<RansWarpSm*>(smem_raw)[warp];
   const int my_g = lane >> 2, my_l = lane & 3;
   const int count = lists->count[0];
   const int ngroups = (count + kGroup - 1) / kGroup;
@@ -402,85 +419,127 @@ dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
     g = __shfl_sync(kFull, g, 0);
     if (g >= ngroups) break;
     const int first = g * kGroup;
-    // tables of the eight shards into shared memory, coarse bucket tables
-    for (int k = 0; k < kGroup; ++k) {
-      const int p = first + k;
-      const bool live = p < count && tables[p].valid;
-      if (lane == 0) sm.valid[k] = live;
-      if (!live) continue;
-      const int n = tables[p].nsym;
-      for (int i = lane; i < n; i += 32) sm.r[k].info[i] = tables[p].info[i];
-      for (int i = lane; i < 128; i += 32) sm.bitmap[i] = 0;
-      __syncwarp();
-      for (int i = 1 + lane; i < n; i += 32) {
-        const uint32_t c = sm.r[k].info[i].x & 0xffffu;
-        atomicOr(&sm.bitmap[c >> 5], 1u << (c & 31));
-      }
-      __syncwarp();
-      uint32_t w[4];
-      int cnt = 0;
+    const int gcount = min(kGroup, count - first);
+    // pool units of shard first + lane (lanes < gcount)
+    int need = 0;
+    if (lane < gcount) {
+      const RansTable& t = tables[first + lane];
+      need = t.valid ? kCoarseUnits + t.nsym : 0;
+    }
+    for (int k = 0; k < gcount;) {
+      // the round: the longest run of shards k.. whose tables fit the pool
+      int inc = lane >= k && lane < gcount ? need : 0;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        w[j] = sm.bitmap[lane * 4 + j];
-        cnt += __popc(w[j]);
-      }
-      int inc = cnt;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
+      for (int o = 1; o < kGroup; o <<= 1) {
         const int v = __shfl_up_sync(kFull, inc, o);
         if (lane >= o) inc += v;
       }
-      int base = inc - cnt;  // symbol starts before this lane's 128 slots
-      uint32_t* cw = reinterpret_cast<uint32_t*>(sm.r[k].coarse) + lane * 4;
+      const uint32_t fits = __ballot_sync(kFull, lane >= k && lane < gcount && inc <= kRansPoolUnits);
+      const int r = max(1, __popc(fits));  // one shard always fits (16 + 255 units)
+      if (lane < kGroup) sm.off[lane] = (lane >= k && lane < k + r && need > 0) ? inc - need : -1;
+      __syncwarp();
+      // tables of the round into the pool, coarse bucket tables
+      uint32_t* bitmap = &sm.rings[0][0];
+      for (int j = k; j < k + r; ++j) {
+        const int off = sm.off[j];
+        if (off < 0) continue;
+        const RansTable& t = tables[first + j];
+        const int n = t.nsym;
+        uint2* info = sm.pool + off + kCoarseUnits;
+        for (int i = lane; i < n; i += 32) info[i] = t.info[i];
+        for (int i = lane; i < 128; i += 32) bitmap[i] = 0;
+        __syncwarp();
+        for (int i = 1 + lane; i < n; i += 32) {
+          const uint32_t c = info[i].x & 0xffffu;
+          atomicOr(&bitmap[c >> 5], 1u << (c & 31));
+        }
+        __syncwarp();
+        // a bucket's first symbol is the number of symbol starts at or
+        // before its first slot; lane L covers bitmap words 4L..4L+3
+        uint32_t w[4];
+        int cnt = 0;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        uint32_t packed = 0;
+        for (int q = 0; q < 4; ++q) {
+          w[q] = bitmap[lane * 4 + q];
+          cnt += __popc(w[q]);
+        }
+        int sc = cnt;
 #pragma unroll
-        for (int h = 0; h < 4; ++h)  // starts at or before the bucket's first slot
-          packed |= static_cast<uint32_t>(base + __popc(w[j] & ((2u << (8 * h)) - 1u))) << (8 * h);
-        cw[j] = packed;
-        base += __popc(w[j]);
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(kFull, sc, o);
+          if (lane >= o) sc += v;
+        }
+        int base = sc - cnt;
+        constexpr int kPerWord = 32 >> kCoarseShift;  // buckets per bitmap word
+        uint32_t packed[kPerWord];                    // this lane's 4 * kPerWord bucket bytes
+#pragma unroll
+        for (int i = 0; i < kPerWord; ++i) packed[i] = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+#pragma unroll
+          for (int h = 0; h < kPerWord; ++h) {
+            const int byte = q * kPerWord + h;
+            const uint32_t upto = (2u << (h << kCoarseShift)) - 1u;  // bits 0 .. first slot of bucket h
+            packed[byte >> 2] |= static_cast<uint32_t>(base + __popc(w[q] & upto)) << (8 * (byte & 3));
+          }
+          base += __popc(w[q]);
+        }
+        uint32_t* cw = reinterpret_cast<uint32_t*>(sm.pool + off) + lane * kPerWord;
+#pragma unroll
+        for (int i = 0; i < kPerWord; ++i) cw[i] = packed[i];
+        __syncwarp();
+      }
+      // decode: lane 4j + l takes lane l of the round's j-th shard
+      const int j = k + my_g;
+      const int off = my_g < r ? sm.off[min(j, kGroup - 1)] : -1;
+      if (off >= 0) {
+        const int p = first + j;
+        const ShardInfo& si = shards[list_items[p]];
+        const FrameDesc& f = frames[si.frame];
+        const uint8_t* body = f.stream + si.offset;
+        uint32_t* out = folded + si.sample_base;
+        const int n = si.count;
+        const uint8_t* coarse = reinterpret_cast<const uint8_t*>(sm.pool + off);
+        const uint2* info = sm.pool + off + kCoarseUnits;
+        uint32_t x = tables[p].state[my_l];
+        const int llen = tables[p].lane_len[my_l];
+        const uint8_t* __restrict__ lb = body + tables[p].lane_start[my_l];
+        int cur = 0;
+        LaneRing ring;
+        ring.init(sm.rings[lane], lb, llen);
+        // Branch-free step: after x = freq*(x>>12) + slot - cum, x >= 2^11, so
+        // renormalisation shifts in one byte when x < 2^23 and a second when
+        // x < 2^15 (decode.cu:540-545), taken from the top of a four-byte
+        // window read ahead of the state chain; two steps use at most four
+        // bytes.  Reading past the lane is an error, found by the byte count.
+        auto step = [&](uint32_t& win, int idx) {
+          const uint32_t slot = x & ((1u << kRansTableLog) - 1u);
+          int sym = coarse[slot >> kCoarseShift];
+          uint2 e = info[sym];
+          while (slot >= (e.y & 0xffffu)) e = info[++sym];
+          out[idx] = e.y >> 16;
+          x = (e.x >> 16) * (x >> kRansTableLog) + slot - (e.x & 0xffffu);
+          const int nb = (x < kRansL) + (x < (kRansL >> 8));
+          x = __funnelshift_l(win, x, 8 * nb);
+          win <<= 8 * nb;
+          cur += nb;
+        };
+        int idx = my_l;
+        for (; idx + 4 < n; idx += 8) {
+          uint32_t win = ring.window(cur);
+          step(win, idx);
+          step(win, idx + 4);
+        }
+        if (idx < n) {
+          uint32_t win = ring.window(cur);
+          step(win, idx);
+        }
+        cp_async_wait<0>();
+        if (cur != llen || x != kRansL) set_status(&state[si.frame].status, 5);
       }
       __syncwarp();
+      k += r;
     }
-    __syncwarp();
-    const int p = first + my_g;
-    if (p < count && sm.valid[my_g]) {
-      const ShardInfo& si = shards[list_items[p]];
-      const FrameDesc& f = frames[si.frame];
-      const uint8_t* body = f.stream + si.offset;
-      uint32_t* out = folded + si.sample_base;
-      const int n = si.count;
-      const RansShardSm& rs = sm.r[my_g];
-      uint32_t x = tables[p].state[my_l];
-      const int llen = tables[p].lane_len[my_l];
-      const uint8_t* __restrict__ lb = body + tables[p].lane_start[my_l];
-      int cur = 0;
-      LaneRing ring;
-      ring.init(sm.rings[lane], lb, llen);
-      // The next two bytes are read one step ahead (their positions do not
-      // depend on the state), so the state chain never waits on memory.
-      uint32_t b0, b1;
-      ring.read2(0, b0, b1);
-      // Branch-free step: after x = freq*(x>>12) + slot - cum, x >= 2^11, so
-      // renormalisation reads one byte when x < 2^23 and a second when
-      // x < 2^15; reading past the lane is an error (decode.cu:540-545).
-      for (int idx = my_l; idx < n; idx += 4) {
-        const uint32_t slot = x & ((1u << kRansTableLog) - 1u);
-        int sym = rs.coarse[slot >> kCoarseShift];
-        uint2 e = rs.info[sym];
-        while (slot >= (e.y & 0xffffu)) e = rs.info[++sym];
-        out[idx] = e.y >> 16;
-        x = (e.x >> 16) * (x >> kRansTableLog) + slot - (e.x & 0xffffu);
-        const int nb = (x < kRansL) + (x < (kRansL >> 8));
-        x = nb == 2 ? (x << 16) | (b0 << 8) | b1 : (nb == 1 ? (x << 8) | b0 : x);
-        cur += nb;
-        ring.read2(cur, b0, b1);
-      }
-      cp_async_wait<0>();
-      if (cur != llen || x != kRansL) set_status(&state[si.frame].status, 5);
-    }
-    __syncwarp();
   }
 }
 
