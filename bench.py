@@ -46,6 +46,11 @@ def parse_args():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
+    p.add_argument("--serve-requests", type=int, default=2000,
+                   help="requests of the serving leg (the serving mix; 0 skips it)")
+    p.add_argument("--serve-rates", default="1000,4000,8000,16000,0",
+                   help="offered request rates of the serving leg, per second (0: all at once)")
+    p.add_argument("--serve-budget-gb", type=float, default=40.0, help="device-memory budget of the server")
     return p.parse_args()
 
 
@@ -62,6 +67,121 @@ def generate(specs, workers):
         return [_gen(s) for s in specs]
     with mp.get_context("spawn").Pool(workers) as pool:
         return pool.map(_gen, specs, chunksize=1)
+
+
+def _gen_serving(key):
+    from fastvid_b200 import synth
+
+    return synth.serving_frame(*key)
+
+
+def serving_leg(args, device):
+    """The serving mix through fastvid_b200.serve.Server (continuous
+    batching) at the offered rates, beside the plain single-frame path on
+    the same request sequence; a sample of answers is compared with the
+    plain path's."""
+    import multiprocessing as mp
+
+    import torch
+
+    import fastvid_b200
+    from fastvid_b200 import synth
+    from fastvid_b200.codec import header_of
+    from fastvid_b200.serve import Server, report, run_open_loop
+
+    per_format = 2
+    keys = [(f, i) for f in range(len(synth.SERVING_FORMATS)) for i in range(per_format)]
+    with mp.get_context("spawn").Pool(min(8, len(keys))) as pool:
+        frames = dict(zip(keys, pool.map(_gen_serving, keys, chunksize=1)))
+    dev = {k: tuple(torch.from_numpy(p).to(device) for p in v) for k, v in frames.items()}
+    params, streams = {}, {}
+    for (f, i), planes in dev.items():
+        fmt = synth.SERVING_FORMATS[f][1]
+        for q in fmt["qualities"]:
+            pr = dict(layout=fmt["layout"], bit_depth=fmt["bit_depth"], quality=q, tile_size=fmt["tile"])
+            params[(f, q)] = pr
+            st = fastvid_b200.encode(planes, **pr)
+            streams[(f, i, q)] = (st, header_of(st))
+    specs = synth.serving_specs(args.serve_requests, frames_per_format=per_format)
+    items, pixels = [], 0
+    for sp in specs:
+        f, i, q = sp["format"], sp["frame"], sp["quality"]
+        fmt = synth.SERVING_FORMATS[f][1]
+        pixels += fmt["width"] * fmt["height"]
+        if sp["kind"] == "encode":
+            items.append(("encode", dev[(f, i)], params[(f, q)]))
+        else:
+            items.append(("decode", streams[(f, i, q)][0], {"header": streams[(f, i, q)][1]}))
+    sample = set(range(0, len(items), 50))
+
+    def plain(item):
+        kind, payload, pr = item
+        if kind == "encode":
+            return fastvid_b200.encode(payload, **pr)
+        return fastvid_b200.decode(payload)
+
+    seen = set()
+    for item in items:  # warm every shape of the plain path
+        key = (item[0], id(item[1]))
+        if key not in seen:
+            seen.add(key)
+            plain(item)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain_answers = {}
+    for j, item in enumerate(items):
+        out = plain(item)
+        if j in sample:
+            plain_answers[j] = out
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+
+    def same(a, b):
+        if isinstance(a, torch.Tensor):
+            return torch.equal(a, b)
+        return len(a) == len(b) and all(torch.equal(x, y) for x, y in zip(a, b))
+
+    rates = [float(r) for r in args.serve_rates.split(",") if r.strip()]
+    out = {"workload": "serving mix: 0.3 720p gray8, 0.4 1080p rgb8 q{100,90,66}, 0.2 4K rgb10 q{100,96,86}, "
+                       "0.1 4K gray16 q{100,87}; 60% encode / 40% decode of streams produced earlier; "
+                       f"{per_format} frames per format, inputs resident in HBM",
+           "requests": len(items), "luma_pixels": pixels, "plain_gpix_s": pixels / plain_s / 1e9,
+           "budget_gb": args.serve_budget_gb, "rates": []}
+    exact = True
+    import gc
+
+    with Server(device, memory_budget=int(args.serve_budget_gb * (1 << 30)), workers=3) as server:
+        run_open_loop(server, items, None)  # grow the resident workspaces to the largest batches
+        for rate in rates:
+            gc.collect()
+            gc.freeze()  # objects made so far are never scanned again: no collector pause mid-run
+            n_batches = len(server.batches)
+            m0 = torch.cuda.memory_stats(device)
+            recs, t0, kept = run_open_loop(server, items, rate or None, seed=int(rate), keep=sample)
+            m1 = torch.cuda.memory_stats(device)
+            gc.unfreeze()
+            rep = report(recs, t0)
+            rep["offered_req_s"] = rate or "all at once"
+            rep["allocator"] = {k: m1.get(k, 0) - m0.get(k, 0) for k in ("num_alloc_retries", "num_device_alloc",
+                                                                         "num_device_free", "num_sync_all_streams")}
+            rep["reserved_gb"] = m1.get("reserved_bytes.all.current", 0) / 2**30
+            runs = server.batch_times[n_batches:]
+            sizes = [n for _, n in server.batches[n_batches:]]
+            rep["batches"] = len(sizes)
+            rep["mean_batch"] = sum(sizes) / max(1, len(sizes))
+            rep["longest_batch_ms"] = max((r[1] - r[0]) * 1e3 for r in runs) if runs else 0.0
+            rep["longest_batches"] = [dict(ms=round((r[1] - r[0]) * 1e3, 2), kind=r[2], frames=r[3], mpix=r[4] / 1e6,
+                                           at_s=round(r[0] - t0, 4))
+                                      for r in sorted(runs, key=lambda r: r[0] - r[1])[:3]]
+            exact = exact and rep["failed"] == 0 and all(same(kept[j], plain_answers[j]) for j in sample)
+            out["rates"].append(rep)
+        out["max_concurrent_batches"] = server.max_concurrent
+        out["mean_batch"] = sum(n for _, n in server.batches) / max(1, len(server.batches))
+    best = max(r["gpix_s"] for r in out["rates"]) if out["rates"] else 0.0
+    out["served_over_plain"] = best / out["plain_gpix_s"]
+    out["bit_exact_sample"] = f"{len(sample)} answers per rate equal to the plain path's: {exact}"
+    out["bit_exact"] = bool(exact)
+    return out
 
 
 def cpu_sample(specs):
@@ -408,6 +528,10 @@ def main():
         gpix, threads, reps = time_oracle(host_frames, specs, idx, args.cpu_seconds)
         line["cpu_baseline"] = {"value": gpix, "unit": "Gpix/s", "cores": threads, "kind": "port",
                                 "sample": f"frames {idx} (one per format), encode+decode, {reps} reps"}
+    # serving form (one GPU): continuous batching at offered rates, p50/p99
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        line["serving"] = serving_leg(args, device)
+        line["bit_exact"] = bool(line["bit_exact"] and line["serving"]["bit_exact"])
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -64,7 +64,12 @@ class BatchCodec:
     but their outputs and issue one graph launch for all analysis passes.
     """
 
-    def __init__(self, device=None, use_graphs: bool = True, max_cached_shapes: int = 8):
+    def __init__(self, device=None, use_graphs: bool = True, max_cached_shapes: int = 8,
+                 resident_workspace: bool = False):
+        """resident_workspace: every batch shape shares one device workspace
+        that grows to the largest batch seen and is kept (a server's
+        steady state allocates no workspace); otherwise each cached shape
+        owns its own."""
         dev = torch.device(device) if device is not None else torch.device("cuda")
         if dev.type != "cuda":
             raise RuntimeError("BatchCodec needs a CUDA device")
@@ -77,6 +82,40 @@ class BatchCodec:
         self._dec_plans: dict = {}
         self._hdr_scratch = None
         self.lib = _native.load()
+        self.resident = resident_workspace
+        self._ws_buf: torch.Tensor | None = None
+        self._pin_buf: torch.Tensor | None = None
+
+    def workspace_bytes(self) -> int:
+        """Device bytes of the resident workspace (0 when not resident)."""
+        return self._ws_buf.numel() if self._ws_buf is not None else 0
+
+    def _results(self, n: int) -> torch.Tensor:
+        """Pinned int64 [n, 2] status/length buffer (shared by every shape
+        in resident mode, where calls run one at a time)."""
+        if not self.resident:
+            return torch.zeros((n, 2), dtype=torch.int64).pin_memory()
+        if self._pin_buf is None or self._pin_buf.size(0) < n:
+            self._pin_buf = torch.zeros((max(n, 64), 2), dtype=torch.int64).pin_memory()
+        return self._pin_buf[:n]
+
+    def release_workspace(self):
+        """Drop the resident workspace (and the shapes cached on it)."""
+        self._enc.clear()
+        self._dec.clear()
+        self._ws_buf = None
+
+    def _workspace(self, nbytes: int) -> torch.Tensor:
+        if not self.resident:
+            return torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        if self._ws_buf is None or self._ws_buf.numel() < nbytes:
+            # cached shapes (and their graphs) point into the old buffer;
+            # calls return only once their work is done, so nothing uses it
+            self._enc.clear()
+            self._dec.clear()
+            self._ws_buf = None
+            self._ws_buf = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8, device=self.device)
+        return self._ws_buf[:nbytes]
 
     # ---- encode -----------------------------------------------------------
     def _encode_slot(self, frames_py: list[Frame]) -> _EncodeSlot:
@@ -89,8 +128,8 @@ class BatchCodec:
         arr = (Frame * n)(*frames_py)
         ws = ctypes.c_int64()
         _native.check(self.lib.fvb_batch_encode_plan(arr, n, ctypes.byref(ws)))
-        workspace = torch.empty(ws.value, dtype=torch.uint8, device=self.device)
-        results = torch.zeros((n, 2), dtype=torch.int64).pin_memory()
+        workspace = self._workspace(ws.value)
+        results = self._results(n)
         slot = _EncodeSlot(arr, n, ws.value, workspace, results)
         if len(self._enc) >= self.max_cached:
             self._enc.pop(next(iter(self._enc)))
@@ -195,8 +234,8 @@ class BatchCodec:
         arr = (Frame * n)(*frames_py)
         ws = ctypes.c_int64()
         _native.check(self.lib.fvb_batch_decode_plan(arr, n, ctypes.byref(ws)))
-        workspace = torch.empty(ws.value, dtype=torch.uint8, device=self.device)
-        results = torch.zeros((n, 2), dtype=torch.int64).pin_memory()
+        workspace = self._workspace(ws.value)
+        results = self._results(n)
         slot = _DecodeSlot(arr, n, ws.value, workspace, results, wavefront)
         if len(self._dec) >= self.max_cached:
             self._dec.pop(next(iter(self._dec)))
@@ -208,8 +247,10 @@ class BatchCodec:
                                                         slot.workspace.data_ptr(), slot.ws_bytes,
                                                         slot.results.data_ptr(), stream_handle))
 
-    def decode(self, streams, predictor="wavefront"):
-        """Decode a list of 1-D uint8 streams; returns a list of plane tuples."""
+    def decode(self, streams, predictor="wavefront", headers=None):
+        """Decode a list of 1-D uint8 streams; returns a list of plane tuples.
+        `headers`: the streams' first 32 bytes when the caller has them
+        (saves reading them back from the device)."""
         if predictor not in ("wavefront", "serial"):
             raise ValueError("predictor must be 'wavefront' or 'serial'")
         n = len(streams)
@@ -228,12 +269,15 @@ class BatchCodec:
             need = ((16 * n + 255) // 256) * 256 + 32 * n
             if self._hdr_scratch is None or self._hdr_scratch.numel() < need:
                 self._hdr_scratch = torch.empty(max(need, 1 << 16), dtype=torch.uint8, device=self.device)
-            heads = ctypes.create_string_buffer(32 * n)
             s_arr = (ctypes.c_void_p * n)(*[s.data_ptr() for s in dev_streams])
             l_arr = (ctypes.c_int64 * n)(*[s.numel() for s in dev_streams])
-            _native.check(self.lib.fvb_gather_headers(s_arr, l_arr, n, self._hdr_scratch.data_ptr(),
-                                                      self._hdr_scratch.numel(), heads, cur.cuda_stream))
-            raw = heads.raw
+            if headers is not None and len(headers) == n and all(len(h) >= 32 for h in headers):
+                raw = b"".join(bytes(h[:32]) for h in headers)
+            else:
+                heads = ctypes.create_string_buffer(32 * n)
+                _native.check(self.lib.fvb_gather_headers(s_arr, l_arr, n, self._hdr_scratch.data_ptr(),
+                                                          self._hdr_scratch.numel(), heads, cur.cuda_stream))
+                raw = heads.raw
             plans = []
             for i, s in enumerate(dev_streams):
                 header = raw[32 * i:32 * i + 32]

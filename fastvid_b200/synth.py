@@ -205,3 +205,42 @@ def reference_pattern(layout: str, width: int, height: int, bit_depth: int, patt
             v = i * (977 + seed * 13) + i * i * 17 + seed * 131
         planes.append((v % (maximum + 1)).astype(np.uint16).reshape(height, pw))
     return tuple(planes)
+
+
+# The serving mix: formats drawn with weights 0.3 720p gray8, 0.4 1080p RGB8,
+# 0.2 4K RGB10, 0.1 4K gray16; quality giving steps {1, 3, 7} (8/10-bit) or
+# {1, 417/556} (16-bit; gray8 is always lossless); 60% encode, 40% decode of
+# streams produced earlier.
+SERVING_FORMATS = [
+    (0.3, dict(width=1280, height=720, layout="gray", bit_depth=8, qualities=(100,), tile=(64, 64))),
+    (0.4, dict(width=1920, height=1080, layout="rgb444", bit_depth=8, qualities=(100, 90, 66), tile=(64, 64))),
+    (0.2, dict(width=3840, height=2160, layout="rgb444", bit_depth=10, qualities=(100, 96, 86), tile=(128, 128))),
+    (0.1, dict(width=3840, height=2160, layout="gray", bit_depth=16, qualities=(100, 87), tile=(128, 128))),
+]
+
+
+def serving_specs(count: int, seed: int = 5, encode_share: float = 0.6, frames_per_format: int = 2):
+    """`count` request specs: dicts with kind, format index, frame index
+    (within that format's pool of `frames_per_format` frames) and quality."""
+    rng = np.random.default_rng(seed)
+    weights = np.array([w for w, _ in SERVING_FORMATS])
+    fmt = rng.choice(len(SERVING_FORMATS), size=count, p=weights / weights.sum())
+    kind = rng.random(count) < encode_share
+    out = []
+    for i in range(count):
+        f = SERVING_FORMATS[int(fmt[i])][1]
+        out.append(dict(kind="encode" if kind[i] else "decode", format=int(fmt[i]),
+                        frame=int(rng.integers(frames_per_format)),
+                        quality=int(f["qualities"][int(rng.integers(len(f["qualities"])))])))
+    return out
+
+
+def serving_frame(fmt: int, index: int, scale: int = 1):
+    """Frame `index` of serving format `fmt` (sizes divided by `scale` for
+    small test runs)."""
+    f = SERVING_FORMATS[fmt][1]
+    depth = f["bit_depth"]
+    return make_frame(f["width"] // scale, f["height"] // scale, f["layout"], depth, 7000 + 97 * fmt + index,
+                      amplitude=20000 if depth == 16 else None, mean=32768 if depth == 16 else None,
+                      rects=20 if depth == 16 else 10,
+                      sigma=(40, 1) if depth == 16 else ((4, 1) if depth == 10 else (3, 1)))
