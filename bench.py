@@ -29,9 +29,9 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = ("mixed96: 32x 1280x720 gray8 q100 tile64, 32x 1920x1080 rgb444-8 q90 tile64, "
-            "16x 3840x2160 rgb444-10 q85 tile128, 16x 2048x1080 gray16 q87 tile128; "
-            "every 4th frame near-flat (noise sd 0.5)")
+WORKLOAD = ("mixed96: 32x 1280x720 gray8 q100, 32x 1920x1080 rgb444-8 q90, "
+            "16x 3840x2160 rgb444-10 q85, 16x 2048x1080 gray16 q87; "
+            "every 4th frame near-flat (noise sd 0.5); tiles in config.tiles")
 TILES = {("gray", 8): (64, 64), ("rgb444", 8): (64, 64), ("rgb444", 10): (128, 128), ("gray", 16): (128, 128)}
 
 
@@ -46,6 +46,7 @@ def parse_args():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
+    p.add_argument("--no-tuning", action="store_true", help="ignore the autotuned table (tiles, launch geometry)")
     p.add_argument("--serve-requests", type=int, default=2000,
                    help="requests of the serving leg (the serving mix; 0 skips it)")
     p.add_argument("--serve-rates", default="1000,4000,8000,16000,0",
@@ -265,7 +266,7 @@ def time_oracle(frames, specs, idx, budget_s):
         for i in idx:
             s = specs[i]
             stream = oracle.encode(frames[i], layout=s["layout"], bit_depth=s["bit_depth"], quality=s["quality"],
-                                   tile_size=TILES[(s["layout"], s["bit_depth"])], threads=threads)
+                                   tile_size=s["tile"], threads=threads)
             oracle.decode(stream, threads=threads)
         total += time.perf_counter() - t0
         reps += 1
@@ -296,7 +297,9 @@ def run_reference(args, specs):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "frames": len(specs), "parallelism": "replicas"},
+        "config": {"workload": WORKLOAD, "frames": len(specs), "parallelism": "replicas",
+                   "tiles": {f"{sp['layout']}-{sp['bit_depth']}-{sp['width']}x{sp['height']}": list(sp["tile"])
+                             for sp in specs}},
         "cpu_baseline": {"value": value, "unit": "Gpix/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -315,8 +318,13 @@ def main():
     from fastvid_b200 import synth
 
     specs = synth.mixed_batch_specs(args.frames)
+    from fastvid_b200 import autotune
+
+    table = autotune.load() if autotune.TABLE.exists() and not args.no_tuning else None
     for s in specs:
-        s["tile"] = TILES[(s["layout"], s["bit_depth"])]
+        s["tile"] = autotune.tile_for(table, s["layout"], s["bit_depth"], s["width"], s["height"],
+                                      default=TILES[(s["layout"], s["bit_depth"])])
+    args.tuning = ("autotuned table fastvid_b200/tuning/b200.json" if table else "built-in defaults")
     if args.impl == "reference":
         return run_reference(args, specs)
 
@@ -335,6 +343,8 @@ def main():
 
     torch.cuda.set_device(local_rank)
     device = torch.device("cuda", local_rank)
+    if table:
+        autotune.apply(table)
     dist = None
     if world > 1:
         import datetime
@@ -448,6 +458,9 @@ def main():
         "data": "synthetic (seeded integer generator standing in for the unavailable corpus)",
         "config": {"workload": WORKLOAD, "frames": len(specs), "luma_pixels": luma, "samples": samples,
                    "form": "batched (one launch per kernel for the whole batch)",
+                   "tiles": {autotune.format_key(sp["layout"], sp["bit_depth"], sp["width"], sp["height"]):
+                             list(sp["tile"]) for sp in specs},
+                   "tuning": args.tuning, "launch_ctas_per_sm": autotune.launch_settings(),
                    "l2": "inputs 1.3 GB > 126 MB L2 (no flush needed)", "parallelism": f"replicas x{world}"},
         "enc_gpix_s": world * luma / (enc_ms / 1e3) / 1e9, "dec_gpix_s": world * luma / (dec_ms / 1e3) / 1e9,
         "enc_ms": enc_ms, "dec_ms": dec_ms, "stream_bytes": stream_bytes, "bit_exact": bool(bit_exact),

@@ -401,6 +401,21 @@ int grid_for(int64_t items, int per_cta, int ctas_per_sm) {
   return static_cast<int>(want < cap ? want : cap);
 }
 
+// Launch geometry of the persistent kernels: the grid is capped at this
+// many CTAs per SM (0: the kernel has no such knob).  Outputs never depend on
+// it -- every such kernel takes its work from a queue or a grid-stride loop.
+constexpr int kDefaultCtas[K_COUNT] = {
+    /*enc_init*/ 0, /*enc_predict*/ 4, /*enc_predict_wide*/ 8, /*enc_analyze*/ 6, /*enc_rans*/ 0,
+    /*enc_scan*/ 0, /*enc_prefix*/ 0, /*enc_emit*/ 8, /*dec_parse*/ 8, /*dec_rans_tables*/ 16,
+    /*dec_reconstruct*/ 4, /*dec_reconstruct_wide*/ 8, /*dec_reconstruct_serial*/ 0, /*results*/ 0,
+    /*dec_rans*/ 16, /*dec_other*/ 16};
+std::atomic<int> g_ctas[K_COUNT];
+
+int ctas(int kernel) {
+  const int v = g_ctas[kernel].load(std::memory_order_relaxed);
+  return v > 0 ? v : kDefaultCtas[kernel];
+}
+
 std::string status_message_encode(int64_t st) {
   if (st == kStatusInternal + 1) return "tile payload is too large";
   char buf[96];
@@ -418,6 +433,19 @@ int fvb_abi_version(void) { return FVB_ABI_VERSION; }
 int64_t fvb_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int fvb_kernel_count(void) { return K_COUNT; }
+
+int fvb_set_launch_ctas(int kernel, int ctas_per_sm) {
+  if (kernel < 0 || kernel >= K_COUNT || kDefaultCtas[kernel] == 0)
+    return fail(FVB_ERR_ARGUMENT, "kernel has no launch-geometry knob");
+  if (ctas_per_sm < 0 || ctas_per_sm > 64) return fail(FVB_ERR_ARGUMENT, "CTAs per SM must be in 0..64");
+  g_ctas[kernel].store(ctas_per_sm, std::memory_order_relaxed);
+  return FVB_OK;
+}
+
+int fvb_get_launch_ctas(int kernel) {
+  if (kernel < 0 || kernel >= K_COUNT || kDefaultCtas[kernel] == 0) return -1;
+  return ctas(kernel);
+}
 
 const char* fvb_kernel_name(int kernel) { return kernel >= 0 && kernel < K_COUNT ? kKernelNames[kernel] : ""; }
 
@@ -564,21 +592,21 @@ int fvb_batch_encode_enqueue(const fvb_frame* frames, int n, void* workspace, in
     FVB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), stream));
     {
       LaunchScope scope_(K_ENC_PREDICT, stream);
-      enc_predict_kernel<<<grid_for(tiles, kWarpsPerCta, 4), kWarpsPerCta * 32, enc_predict_smem(), stream>>>(
+      enc_predict_kernel<<<grid_for(tiles, kWarpsPerCta, ctas(K_ENC_PREDICT)), kWarpsPerCta * 32, enc_predict_smem(), stream>>>(
           frames_d, state, nf, tiles, shards, folded, queue);
     }
     FVB_LAUNCHED("enc_predict_kernel");
     if (t.wide) {
       {
         LaunchScope scope_(K_ENC_PREDICT_WIDE, stream);
-        enc_predict_wide_kernel<<<grid_for(tiles, 1, 8), 256, 0, stream>>>(frames_d, state, nf, tiles, folded, recon);
+        enc_predict_wide_kernel<<<grid_for(tiles, 1, ctas(K_ENC_PREDICT_WIDE)), 256, 0, stream>>>(frames_d, state, nf, tiles, folded, recon);
       }
       FVB_LAUNCHED("enc_predict_wide_kernel");
     }
     {
       // resident CTAs only: each warp streams its shards through one ring
       LaunchScope scope_(K_ENC_ANALYZE, stream);
-      enc_analyze_kernel<<<grid_for(nsh, kWarpsPerCta, 6), kWarpsPerCta * 32, 0, stream>>>(frames_d, state, nf, shards,
+      enc_analyze_kernel<<<grid_for(nsh, kWarpsPerCta, ctas(K_ENC_ANALYZE)), kWarpsPerCta * 32, 0, stream>>>(frames_d, state, nf, shards,
                                                                                            nsh, folded, rans);
     }
     FVB_LAUNCHED("enc_analyze_kernel");
@@ -633,7 +661,7 @@ int fvb_batch_encode_emit(const fvb_frame* frames, int n, void* workspace, int64
   FVB_LAUNCHED("enc_prefix_kernel");
   {
     LaunchScope scope_(K_ENC_EMIT, stream);
-    enc_emit_kernel<<<grid_for(t.shards, kWarpsPerCta, 8), kWarpsPerCta * 32, enc_emit_smem(), stream>>>(
+    enc_emit_kernel<<<grid_for(t.shards, kWarpsPerCta, ctas(K_ENC_EMIT)), kWarpsPerCta * 32, enc_emit_smem(), stream>>>(
         frames_d, n, reinterpret_cast<const ShardInfo*>(ws + L.shards), t.shards,
         reinterpret_cast<const uint32_t*>(ws + L.folded), reinterpret_cast<const uint8_t*>(ws + L.rans), outs_d);
   }
@@ -828,41 +856,41 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
   FVB_CUDA(cudaMemsetAsync(lists, 0, sizeof(DecodeLists), stream));
   {
     LaunchScope scope_(K_DEC_PARSE, stream);
-    dec_parse_kernel<<<grid_for(t.tiles, 128, 8), 128, 0, stream>>>(frames_d, state, n, t.tiles, shards, t.shards,
+    dec_parse_kernel<<<grid_for(t.tiles, 128, ctas(K_DEC_PARSE)), 128, 0, stream>>>(frames_d, state, n, t.tiles, shards, t.shards,
                                                                        lists, items);
   }
   FVB_LAUNCHED("dec_parse_kernel");
   RansTable* tables = reinterpret_cast<RansTable*>(ws + L.tables);
   {
     LaunchScope scope_(K_DEC_SHARDS, stream);
-    dec_rans_tables_kernel<<<grid_for(t.shards, 128, 16), 128, 0, stream>>>(frames_d, state, shards, lists, items,
+    dec_rans_tables_kernel<<<grid_for(t.shards, 128, ctas(K_DEC_SHARDS)), 128, 0, stream>>>(frames_d, state, shards, lists, items,
                                                                            tables);
   }
   FVB_LAUNCHED("dec_rans_tables_kernel");
   {
     LaunchScope scope_(K_DEC_RANS, stream);
-    dec_rans_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), kWarpsPerCta, 16), kWarpsPerCta * 32, dec_rans_smem(),
+    dec_rans_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), kWarpsPerCta, ctas(K_DEC_RANS)), kWarpsPerCta * 32, dec_rans_smem(),
                       stream>>>(
         frames_d, state, shards, lists, items, tables, folded);
   }
   FVB_LAUNCHED("dec_rans_kernel");
   {
     LaunchScope scope_(K_DEC_OTHER, stream);
-    dec_other_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), 4, 16), 128, 0, stream>>>(
+    dec_other_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), 4, ctas(K_DEC_OTHER)), 128, 0, stream>>>(
         frames_d, state, shards, t.shards, lists, items, folded);
   }
   FVB_LAUNCHED("dec_other_kernel");
   if (wavefront) {
     {
       LaunchScope scope_(K_DEC_RECON, stream);
-      dec_reconstruct_kernel<<<grid_for(t.tiles, kWarpsPerCta, 4), kWarpsPerCta * 32, dec_reconstruct_smem(), stream>>>(
+      dec_reconstruct_kernel<<<grid_for(t.tiles, kWarpsPerCta, ctas(K_DEC_RECON)), kWarpsPerCta * 32, dec_reconstruct_smem(), stream>>>(
           frames_d, state, n, t.tiles, folded, queue);
     }
     FVB_LAUNCHED("dec_reconstruct_kernel");
     if (t.wide) {
       {
         LaunchScope scope_(K_DEC_RECON_WIDE, stream);
-        dec_reconstruct_wide_kernel<<<grid_for(t.tiles, 1, 8), 256, 0, stream>>>(frames_d, state, n, t.tiles, folded);
+        dec_reconstruct_wide_kernel<<<grid_for(t.tiles, 1, ctas(K_DEC_RECON_WIDE)), 256, 0, stream>>>(frames_d, state, n, t.tiles, folded);
       }
       FVB_LAUNCHED("dec_reconstruct_wide_kernel");
     }

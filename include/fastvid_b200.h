@@ -64,6 +64,15 @@ int64_t fvb_launch_count(void);
 /* Kernel identifiers 0..fvb_kernel_count()-1 and their names. */
 int fvb_kernel_count(void);
 const char* fvb_kernel_name(int kernel);
+
+/* Launch geometry of a persistent kernel (no counterpart in the reference;
+ * the knob the autotuner sets): its grid is capped at `ctas_per_sm` CTAs per
+ * SM, 0 restoring the built-in default.  Process-wide, read at each launch;
+ * no output depends on it.  FVB_ERR_ARGUMENT for a kernel without the knob
+ * or a value outside 0..64. */
+int fvb_set_launch_ctas(int kernel, int ctas_per_sm);
+/* The cap in effect, or -1 for a kernel without the knob. */
+int fvb_get_launch_ctas(int kernel);
 /* While profiling is on (per calling thread), every launch is bracketed by
  * CUDA events on its stream; fvb_profile_end waits for them and writes, per
  * kernel id, the summed milliseconds and the number of launches. */

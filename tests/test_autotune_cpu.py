@@ -1,0 +1,68 @@
+"""CPU tests of the autotuner's selection rules and of the launch-geometry
+knob of the C ABI (host-side state only, no kernel launch)."""
+
+import pytest
+
+from fastvid_b200 import _native, autotune
+
+
+def test_choose_tile_takes_the_fastest_within_the_size_tolerance():
+    res = {(32, 32): (1.0, 1100), (64, 64): (1.5, 1010), (128, 128): (2.0, 1000)}
+    assert autotune.choose_tile(res, 0.02) == (64, 64)   # 32x32 is 10% larger
+    assert autotune.choose_tile(res, 0.2) == (32, 32)
+    assert autotune.choose_tile(res, 0.0) == (128, 128)
+    tie = {(32, 32): (1.0, 1005), (64, 64): (1.0, 1000)}
+    assert autotune.choose_tile(tie, 0.01) == (64, 64)   # equal time: the smaller stream
+
+
+def test_descend_finds_the_separable_optimum():
+    target = {"a": 6, "b": 3}
+    calls = []
+
+    def cost(s):
+        calls.append(dict(s))
+        return 10 + (s["a"] - target["a"]) ** 2 + (s["b"] - target["b"]) ** 2
+
+    best = autotune.descend(("a", "b"), (2, 3, 4, 6, 8), cost, {"a": 2, "b": 8})
+    assert best == target
+    assert len(calls) < 30
+
+
+def test_descend_keeps_the_start_without_a_real_gain():
+    best = autotune.descend(("a",), (1, 2, 3), lambda s: 100.0 - 0.1 * s["a"], {"a": 1}, min_gain=0.01)
+    assert best == {"a": 1}
+
+
+def test_launch_knob_round_trip_and_rejections():
+    lib = _native.load()
+    names = _native.kernel_names()
+    before = autotune.launch_settings()
+    assert set(autotune.LAUNCH_KNOBS) <= set(before)
+    try:
+        autotune.set_launch({"enc_predict": 3, "dec_rans": 12})
+        now = autotune.launch_settings()
+        assert now["enc_predict"] == 3 and now["dec_rans"] == 12
+        autotune.reset_launch()
+        assert autotune.launch_settings() == before
+        assert lib.fvb_set_launch_ctas(names.index("enc_rans"), 4) != 0
+        assert _native.last_error() == "kernel has no launch-geometry knob"
+        assert lib.fvb_get_launch_ctas(names.index("enc_rans")) == -1
+        assert lib.fvb_set_launch_ctas(names.index("enc_predict"), 65) != 0
+        with pytest.raises(RuntimeError):
+            autotune.set_launch({"enc_scan": 2})
+    finally:
+        autotune.reset_launch()
+
+
+def test_table_round_trip(tmp_path):
+    table = {"tiles": {autotune.format_key("gray", 8, 1280, 720): [32, 32]}, "launch": {"enc_emit": 6}}
+    path = tmp_path / "t.json"
+    autotune.save(table, path)
+    assert autotune.load(path) == table
+    assert autotune.tile_for(table, "gray", 8, 1280, 720) == (32, 32)
+    assert autotune.tile_for(table, "gray", 8, 640, 480, default=(64, 64)) == (64, 64)
+    try:
+        autotune.apply(table)
+        assert autotune.launch_settings()["enc_emit"] == 6
+    finally:
+        autotune.reset_launch()
