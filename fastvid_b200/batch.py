@@ -41,6 +41,7 @@ class _EncodeSlot:
     results: torch.Tensor            # pinned int64 [n, 2]
     graph: torch.cuda.CUDAGraph | None = None
     stream: torch.cuda.Stream | None = None
+    kernels: int = 0                 # kernel launches captured in the graph
     last_ptrs: tuple = field(default_factory=tuple)
 
 
@@ -54,6 +55,7 @@ class _DecodeSlot:
     wavefront: bool
     graph: torch.cuda.CUDAGraph | None = None
     stream: torch.cuda.Stream | None = None
+    kernels: int = 0
 
 
 class BatchCodec:
@@ -85,6 +87,7 @@ class BatchCodec:
         self.resident = resident_workspace
         self._ws_buf: torch.Tensor | None = None
         self._pin_buf: torch.Tensor | None = None
+        self.graph_kernels = 0  # kernels run by graph replays (launch_count() sees only direct launches)
 
     def workspace_bytes(self) -> int:
         """Device bytes of the resident workspace (0 when not resident)."""
@@ -194,13 +197,16 @@ class BatchCodec:
                         self._enqueue_encode(slot, slot.stream.cuda_stream)
                     slot.stream.synchronize()
                     graph = torch.cuda.CUDAGraph()
+                    k0 = _native.launch_count()
                     with torch.cuda.graph(graph, stream=slot.stream):
                         self._enqueue_encode(slot, slot.stream.cuda_stream)
+                    slot.kernels = _native.launch_count() - k0
                     slot.graph = graph
                     cur.wait_stream(slot.stream)
                 slot.stream.wait_stream(cur)
                 with torch.cuda.stream(slot.stream):
                     slot.graph.replay()
+                self.graph_kernels += slot.kernels
                 slot.stream.synchronize()
                 cur.wait_stream(slot.stream)
             else:
@@ -213,14 +219,17 @@ class BatchCodec:
             lengths = [length for _, length in res]
             total = sum(lengths)
             arena = torch.empty(total, dtype=torch.uint8, device=self.device)
-            outs, views, off = [], [], 0
+            outs, off, base = [], 0, arena.data_ptr()
             for length in lengths:
-                views.append(arena.narrow(0, off, length))
-                outs.append(arena.data_ptr() + off)
+                outs.append(base + off)
                 off += length
             o_arr = (ctypes.c_void_p * n)(*outs)
             _native.check(self.lib.fvb_batch_encode_emit(slot.frames, n, slot.workspace.data_ptr(), slot.ws_bytes,
                                                          o_arr, cur.cuda_stream))
+            views, off = [], 0  # made while the GPU emits
+            for length in lengths:
+                views.append(arena.narrow(0, off, length))
+                off += length
         return views
 
     # ---- decode -----------------------------------------------------------
@@ -290,18 +299,32 @@ class BatchCodec:
             slot = self._decode_slot(plans, predictor == "wavefront")
             total = sum(f.samples for f in plans)
             arena = torch.empty(total, dtype=torch.uint16, device=self.device)
-            out_planes, ptrs, pitches, off = [], [], [], 0
+            # plane pointers by arithmetic (Y, then Cb, then Cr of each frame);
+            # the tensor views are made while the GPU decodes
+            ptrs, pitches, off, base = [], [], 0, arena.data_ptr()
             for f in plans:
-                pv = plane_views(arena.narrow(0, off, f.samples), f)
+                y = f.width * f.height
+                if f.planes == 3:
+                    cw = f.plane_width[1]
+                    c = cw * f.height
+                    ptrs.extend([base + 2 * off, base + 2 * (off + y), base + 2 * (off + y + c)])
+                    pitches.extend([f.width, cw, cw])
+                else:
+                    ptrs.extend([base + 2 * off, 0, 0])
+                    pitches.extend([f.width, 0, 0])
                 off += f.samples
-                out_planes.append(tuple(pv))
-                ptrs.extend([p.data_ptr() for p in pv] + [0] * (3 - len(pv)))
-                pitches.extend([p.size(1) for p in pv] + [0] * (3 - len(pv)))
             p_arr = (ctypes.c_void_p * (3 * n))(*ptrs)
             q_arr = (ctypes.c_int64 * (3 * n))(*pitches)
             _native.check(self.lib.fvb_batch_decode_prepare(slot.frames, n, s_arr, l_arr, p_arr, q_arr,
                                                             slot.workspace.data_ptr(), slot.ws_bytes,
                                                             cur.cuda_stream))
+            def views():
+                out, off = [], 0
+                for f in plans:
+                    out.append(tuple(plane_views(arena.narrow(0, off, f.samples), f)))
+                    off += f.samples
+                return out
+
             if self.use_graphs:
                 if slot.graph is None:
                     slot.stream = torch.cuda.Stream(self.device)
@@ -310,8 +333,10 @@ class BatchCodec:
                         self._enqueue_decode(slot, slot.stream.cuda_stream)
                     slot.stream.synchronize()
                     graph = torch.cuda.CUDAGraph()
+                    k0 = _native.launch_count()
                     with torch.cuda.graph(graph, stream=slot.stream):
                         self._enqueue_decode(slot, slot.stream.cuda_stream)
+                    slot.kernels = _native.launch_count() - k0
                     slot.graph = graph
                     cur.wait_stream(slot.stream)
                     # the eager run above already decoded this batch
@@ -319,10 +344,13 @@ class BatchCodec:
                     slot.stream.wait_stream(cur)
                     with torch.cuda.stream(slot.stream):
                         slot.graph.replay()
+                    self.graph_kernels += slot.kernels
+                out_planes = views()
                 slot.stream.synchronize()
                 cur.wait_stream(slot.stream)
             else:
                 self._enqueue_decode(slot, cur.cuda_stream)
+                out_planes = views()
                 cur.synchronize()
             for i, (status, _) in enumerate(slot.results.tolist()):
                 if status:
