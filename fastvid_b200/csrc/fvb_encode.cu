@@ -269,6 +269,32 @@ __device__ __forceinline__ uint32_t bit_or_zero(uint32_t s) {
   return r;
 }
 
+// rANS encoding of a symbol with frequency f and start cum maps the state x
+// (below f * 2^19 after renormalisation, so below 2^31) to
+// (x / f) * 4096 + x % f + cum = x + cum + (x / f) * (4096 - f).  The quotient
+// comes from a multiply-high and a shift by an exact reciprocal (Alverson,
+// "Integer division using reciprocals", ARITH 1991): with s = ceil(log2 f)
+// and m = ceil(2^(31+s) / f) < 2^32, floor(x * m / 2^(31+s)) = floor(x / f)
+// for every x < 2^31, because m exceeds 2^(31+s)/f by less than one, which
+// moves x * m / 2^(31+s) by less than x / 2^(31+s) < 2^-s <= 1/f.  For f = 1
+// the multiplier 2^32-1 yields x - 1, and the bias carries the missing 4095.
+// Table entry: the multiplier, then bias | (4096 - f) << 13 | (s - 1) << 25.
+__device__ __forceinline__ uint32_t rans_multiplier(uint32_t f) {
+  if (f < 2) return 0xffffffffu;
+  const uint32_t s = 32 - __clz(f - 1);
+  // m = floor((2^(31+s) - 1) / f) + 1 by long division in 16-bit digits:
+  // 2^(31+s) - 1 = (2^(s-1) - 1) * 2^32 + 0xffffffff, and 2^(s-1) - 1 < f
+  const uint32_t t1 = (((1u << (s - 1)) - 1u) << 16) | 0xffffu;
+  const uint32_t q1 = t1 / f;
+  const uint32_t t2 = ((t1 - q1 * f) << 16) | 0xffffu;
+  return ((q1 << 16) | (t2 / f)) + 1u;
+}
+__device__ __forceinline__ uint32_t rans_packed(uint32_t f, uint32_t cum) {
+  const uint32_t bias = f < 2 ? cum + 4095u : cum;
+  const uint32_t sh = f < 2 ? 0u : 31u - __clz(f - 1);  // s - 1
+  return bias | ((4096u - f) << 13) | (sh << 25);
+}
+
 // Zero-run token statistics of one 128-symbol block (encode.cu:232-240): a
 // run of zeros costs varint(2(run-1)), one byte up to 64 zeros and two beyond
 // (a shard holds at most 4096 symbols).  zm: this lane's zero components at
@@ -705,12 +731,8 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
           if (lane >= o) binc += t;
         }
         if (ok) {
-          // floor(2^32 / fr): floor((2^32-1) / fr), plus one when fr is a
-          // power of two; 2^32 - 1 for fr = 1
-          const uint32_t recip =
-              fr == 1 ? 0xffffffffu : 0xffffffffu / fr + ((fr & (fr - 1)) == 0 ? 1u : 0u);
-          tab[2 * v] = (fr << 16) | static_cast<uint32_t>(pe);
-          tab[2 * v + 1] = recip;
+          tab[2 * v] = rans_multiplier(fr);
+          tab[2 * v + 1] = rans_packed(fr, static_cast<uint32_t>(pe));
           uint32_t cursor = c_cursor + binc - bytes;
           uint32_t d = dv;
           do {
@@ -759,20 +781,6 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
 // shards per warp.  Lane bytes are written back to front so they end up in
 // stream order (the reference reverses them at emission, encode.cu:609).
 
-// Division of a rANS state x < 2^31 by a frequency f <= 4096: q' = mulhi(x, m)
-// with m = floor(2^32 / f) (m = 2^32 - 1 for f = 1) is floor(x / f) or one
-// less, since x*m/2^32 > x/f - x/2^32 > x/f - 1; one compare fixes it and
-// yields the remainder as well (reciprocal division with a correction step,
-// Granlund & Montgomery, PLDI 1994).
-__device__ __forceinline__ void div_freq(uint32_t x, uint32_t f, uint32_t m, uint32_t& q, uint32_t& r) {
-  q = __umulhi(x, m);
-  r = x - q * f;
-  if (r >= f) {
-    ++q;
-    r -= f;
-  }
-}
-
 __global__ void __launch_bounds__(128)
 enc_rans_kernel(const FrameState* __restrict__ state, ShardInfo* __restrict__ shards, int64_t total_shards,
                 const uint32_t* __restrict__ folded, uint8_t* __restrict__ rans_scratch) {
@@ -793,36 +801,38 @@ enc_rans_kernel(const FrameState* __restrict__ state, ShardInfo* __restrict__ sh
   int nacc = 0, nwords = 0;
   const int first = n - 1 - ((n - 1 - lane) & 3);
   const int steps = first >= 0 ? first / 4 + 1 : 0;  // symbols first, first-4, ..., >= 0
+  // one encoding step (encode.cu:401-418): renormalise -- at most two bytes,
+  // since x < 2^31 and the threshold f * 2^19 >= 2^19 -- then the state map
+  auto step = [&](uint2 e) {
+    const uint32_t cmpl = (e.y >> 13) & 0xfffu;
+    const uint32_t thr = (4096u - cmpl) << 19;  // ((L >> 12) << 8) * f
+    const uint32_t b1 = x >= thr, b2 = (x >> 8) >= thr;
+    const int nb = static_cast<int>(b1 + b2);
+    const uint32_t bytes = b2 ? __byte_perm(x, 0, 0x4401) : (x & 0xffu);  // first byte on top
+    acc = (acc << (8 * nb)) | (nb ? bytes : 0u);
+    nacc += nb;
+    if (nacc >= 4) {
+      nacc -= 4;
+      out_end[-(++nwords)] = static_cast<uint32_t>(acc >> (8 * nacc));
+    }
+    x >>= 8 * nb;
+    const uint32_t q = __umulhi(x, e.x) >> (e.y >> 25);
+    x += (e.y & 0x1fffu) + q * cmpl;
+  };
+  // symbols and table entries are loaded eight steps ahead of the state chain
   constexpr int kAhead = 8;
-  for (int c = 0; c < steps; c += kAhead) {
+  int c = 0;
+  for (; c + kAhead <= steps; c += kAhead) {
     uint32_t v[kAhead];
     uint2 e[kAhead];
 #pragma unroll
-    for (int j = 0; j < kAhead; ++j) v[j] = (c + j < steps) ? __ldg(f + first - 4 * (c + j)) : 0u;
+    for (int j = 0; j < kAhead; ++j) v[j] = __ldg(f + first - 4 * (c + j));
 #pragma unroll
-    for (int j = 0; j < kAhead; ++j) e[j] = (c + j < steps) ? tab[v[j]] : make_uint2(1u << 16, 0u);
+    for (int j = 0; j < kAhead; ++j) e[j] = tab[v[j]];
 #pragma unroll
-    for (int j = 0; j < kAhead; ++j) {
-      if (c + j < steps) {
-        const uint32_t fr = e[j].x >> 16, cum = e[j].x & 0xffffu;
-        const uint32_t thr = fr << 19;  // ((L >> 12) << 8) * freq
-        // renormalise: at most two bytes, since x < 2^31 and thr >= 2^19
-        const uint32_t b1 = x >= thr, b2 = (x >> 8) >= thr;
-        const int nb = static_cast<int>(b1 + b2);
-        const uint64_t bytes = b2 ? (((x & 0xffu) << 8) | ((x >> 8) & 0xffu)) : (x & 0xffu);
-        acc = (acc << (8 * nb)) | (nb ? bytes : 0u);
-        nacc += nb;
-        if (nacc >= 4) {
-          nacc -= 4;
-          out_end[-(++nwords)] = static_cast<uint32_t>(acc >> (8 * nacc));
-        }
-        x >>= 8 * nb;
-        uint32_t q, r;
-        div_freq(x, fr, e[j].y, q, r);
-        x = (q << kRansTableLog) + r + cum;
-      }
-    }
+    for (int j = 0; j < kAhead; ++j) step(e[j]);
   }
+  for (; c < steps; ++c) step(tab[__ldg(f + first - 4 * c)]);
   if (nacc) out_end[-(nwords + 1)] = static_cast<uint32_t>(acc << (8 * (4 - nacc)));  // low bytes unused
   si.rans_lane[lane] = 4 * nwords + nacc;
   si.rans_state[lane] = x;
