@@ -146,18 +146,17 @@ __global__ void dec_parse_kernel(const FrameDesc* __restrict__ frames, FrameStat
 //                    zero-run shard g on lane 4g (decode.cu:237-295), block
 //                    shards one after another warp-wide (decode.cu:342-396)
 
-// Measured on the 48-frame mix: 32-slot buckets, 16-word rings and a 3 KB
-// pool beat 8- and 16-slot buckets, 8-word rings and a one-ahead symbol
-// lookup (1.51 ms against 1.51-1.68 ms).
+// Measured on the 48-frame mix: 32-slot buckets beat 8- and 16-slot buckets
+// and a one-ahead symbol lookup.
 constexpr int kGroup = 8;        // shards per warp
 constexpr int kCoarseShift = 5;  // coarse bucket = 32 slots
-constexpr int kRingWords = 16;   // words of a lane's byte ring
 
 struct RansTable {
   int32_t lane_start[4], lane_len[4];
   uint32_t state[4];
   int32_t nsym, valid;
   int32_t pad[2];
+  uint32_t coarse[32];  // first symbol of each 32-slot bucket, one byte per bucket
   uint2 info[256];  // x: cum | freq << 16, y: (cum + freq) | value << 16 (value as u16, decode.cu:484)
 };
 
@@ -231,29 +230,30 @@ struct ByteWindow {
 };
 
 
-// A lane's byte stream through a private ring of kRingWords words in shared
-// memory, fed by cp.async kRingWords/4 words at a time and kept at least
-// 3/4 of the ring ahead of the read position: reads are shared-memory loads
-// whose data arrived long before.  Word w of the aligned range lives in slot
-// w % kRingWords; only words holding a byte of the lane are copied (others
-// keep stale bytes, and reading them is an overrun that the byte count check
-// reports).
+// A lane's byte stream through a private ring of 16 words in shared memory,
+// fed by cp.async four words at a time and kept at least 12 words ahead of
+// the read position: reads are shared-memory loads whose data arrived long
+// before.  Word w of the aligned range lives in slot w % 16; slot s of lane l
+// is word s * 32 + l of the warp's ring block, so every lane reads and fills
+// its own bank whatever its position.  Only words holding a byte of the lane
+// are copied (others keep stale bytes, and reading them is an overrun that
+// the byte count check reports).
 struct LaneRing {
-  static constexpr int kStep = kRingWords / 4;  // words per commit group
-  uint32_t* ring;          // kRingWords words of shared memory
+  static constexpr int kWords = 16;
+  uint32_t* ring;          // slot 0 of this lane (slots 32 words apart)
   const uint32_t* words;   // aligned base of the lane's bytes
   int head;                // lane byte 0 = byte `head` of word 0
   int last;                // last word holding a lane byte (-1: none)
-  int fetched;             // words issued so far
+  int fetched;             // words issued so far (multiple of 4)
 
   __device__ void fetch() {
 #pragma unroll
-    for (int j = 0; j < kStep; ++j) {
+    for (int j = 0; j < 4; ++j) {
       const int w = fetched + j;
-      if (w <= last) cp_async4(ring + (w & (kRingWords - 1)), words + w);
+      if (w <= last) cp_async4(ring + (w & (kWords - 1)) * 32, words + w);
     }
     cp_async_commit();
-    fetched += kStep;
+    fetched += 4;
   }
   __device__ void init(uint32_t* ring_smem, const uint8_t* p, int len) {
     const uintptr_t a = reinterpret_cast<uintptr_t>(p);
@@ -268,14 +268,14 @@ struct LaneRing {
   }
   // The four bytes at lane positions cur..cur+3, first byte in the top bits;
   // cur advances by at most four between calls.  After a fetch the ring
-  // holds words w .. w + 3/4 ring - 1 or more; all but the newest group are
-  // complete, which covers words w and w + 1.
+  // holds words w .. w+11 or more; all but the newest group are complete,
+  // which covers words w and w + 1.
   __device__ uint32_t window(int cur) {
     const int pos = head + cur;
     const int w = pos >> 2;
-    if (fetched - w < 3 * kStep) fetch();
+    if (fetched - w < 12) fetch();
     cp_async_wait<1>();  // the newest group may stay in flight
-    const uint32_t lo = ring[w & (kRingWords - 1)], hi = ring[(w + 1) & (kRingWords - 1)];
+    const uint32_t lo = ring[(w & (kWords - 1)) * 32], hi = ring[((w + 1) & (kWords - 1)) * 32];
     return __byte_perm(__funnelshift_r(lo, hi, 8 * (pos & 3)), 0, 0x0123);
   }
 };
@@ -375,33 +375,92 @@ dec_rans_tables_kernel(const FrameDesc* __restrict__ frames, FrameState* __restr
       const FrameDesc& f = frames[si.frame];
       ok = rans_parse_serial(f.stream + si.offset, si.body, static_cast<uint32_t>(f.max_sample) * 2u, t);
       if (!ok) set_status(&st.status, 5);
+      if (ok) {
+        // bucket b (slots 32b..32b+31) starts in the last symbol whose
+        // cumulative start is at or before slot 32b
+        const int n = t.nsym;
+        int sym = 0;
+        for (int w = 0; w < 32; ++w) {
+          uint32_t packed = 0;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const uint32_t first_slot = static_cast<uint32_t>(w * 4 + q) << kCoarseShift;
+            while (sym + 1 < n && (t.info[sym + 1].x & 0xffffu) <= first_slot) ++sym;
+            packed |= static_cast<uint32_t>(sym) << (8 * q);
+          }
+          t.coarse[w] = packed;
+        }
+      }
     }
     t.valid = ok;
   }
 }
 
-// Shared memory of one dec_rans warp.  A round's tables sit back to back in
-// `pool`: per shard a coarse table (first symbol of each 32-slot bucket,
-// 128 bytes) followed by its nsym info entries -- a few hundred bytes for the
-// handful of symbols a predicted shard holds, so many warps fit on an SM.  A group of eight shards whose tables exceed the pool is decoded in
-// several rounds.
-constexpr int kRansPoolUnits = 384;  // uint2 units: 3 KB
-constexpr int kCoarseBuckets = (1 << kRansTableLog) >> kCoarseShift;
-constexpr int kCoarseUnits = kCoarseBuckets / 8;
+// Shared memory of one dec_rans warp: the eight 4-lane groups' tables,
+// interleaved -- unit u (8 bytes) of group j at pool[u * 8 + j], so lookups
+// of different groups fall in different banks -- and the lanes' byte rings.
+// A group's column holds its shard's 128-entry coarse table (16 units) and up
+// to 40 info entries: the handful of symbols a predicted shard holds.
+// Shards with more symbols are decoded from their table in global memory.
+constexpr int kColumns = 8;                    // 4-lane groups per warp
+constexpr int kColumnUnits = 56;               // 16 coarse + 40 info
+constexpr int kCoarseUnits = (1 << kRansTableLog) >> kCoarseShift >> 3;
+constexpr int kColumnSymbols = kColumnUnits - kCoarseUnits;
 
 struct RansWarpSm {
-  uint2 pool[kRansPoolUnits];
-  // per-lane byte rings; a row one word longer than the ring puts equal
-  // ring slots of different lanes in different banks.  While tables are
-  // built (no decode in flight) the first 128 words hold the symbol-start
-  // bitmap.
-  uint32_t rings[32][kRingWords + 1];
-  int32_t off[kGroup];  // pool offset of each shard of the round (-1: not decoded)
+  uint2 pool[kColumns * kColumnUnits];
+  // per-lane byte rings, slot-major: rings[s][lane]
+  uint32_t rings[LaneRing::kWords][32];
 };
-static_assert(32 * (kRingWords + 1) >= 128, "bitmap alias");
 
 size_t dec_rans_smem() { return sizeof(RansWarpSm) * kWarpsPerCta; }
 
+// Decode lane `my_l` of one shard: n symbols, this lane's byte range `lb`
+// (llen bytes), initial state x; the shard's coarse table and info entries
+// at a stride of 2^LOG_S units.  Returns the bytes consumed and the final
+// state.
+template <int LOG_S>
+__device__ __forceinline__ void rans_decode_lane(const uint8_t* __restrict__ coarse_col, const uint2* __restrict__ info_col,
+                                                 uint32_t* ring_smem, const uint8_t* __restrict__ lb, int llen,
+                                                 uint32_t* __restrict__ out, int n, int my_l, uint32_t& x, int& cur) {
+  LaneRing ring;
+  ring.init(ring_smem, lb, llen);
+  cur = 0;
+  // Branch-free step: after x = freq*(x>>12) + slot - cum, x >= 2^11, so
+  // renormalisation shifts in one byte when x < 2^23 and a second when
+  // x < 2^15 (decode.cu:540-545), taken from the top of a four-byte window
+  // read ahead of the state chain; two steps use at most four bytes.
+  // Reading past the lane is an error, found by the byte count.
+  auto step = [&](uint32_t& win, int idx) {
+    const uint32_t slot = x & ((1u << kRansTableLog) - 1u);
+    const uint32_t b = slot >> kCoarseShift;
+    int sym = coarse_col[((b >> 3) << (LOG_S + 3)) + (b & 7)];
+    uint2 e = info_col[sym << LOG_S];
+    while (slot >= (e.y & 0xffffu)) e = info_col[(++sym) << LOG_S];
+    out[idx] = e.y >> 16;
+    x = (e.x >> 16) * (x >> kRansTableLog) + slot - (e.x & 0xffffu);
+    const int nb = (x < kRansL) + (x < (kRansL >> 8));
+    x = __funnelshift_l(win, x, 8 * nb);
+    win <<= 8 * nb;
+    cur += nb;
+  };
+  int idx = my_l;
+  for (; idx + 4 < n; idx += 8) {
+    uint32_t win = ring.window(cur);
+    step(win, idx);
+    step(win, idx + 4);
+  }
+  if (idx < n) {
+    uint32_t win = ring.window(cur);
+    step(win, idx);
+  }
+  cp_async_wait<0>();
+}
+
+// Each 4-lane group streams rANS shards: it claims the next shard from the
+// list, copies the shard's tables into its column and decodes its four
+// lanes, then claims another -- so every lane stays busy until the list is
+// done, whatever the mix of shards.
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
 dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
                 const ShardInfo* __restrict__ shards, DecodeLists* __restrict__ lists,
@@ -410,136 +469,39 @@ dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   RansWarpSm& sm = reinterpret_cast<RansWarpSm*>(smem_raw)[warp];
-  const int my_g = lane >> 2, my_l = lane & 3;
+  const int j = lane >> 2, my_l = lane & 3;
+  const unsigned group = 0xfu << (4 * j);
   const int count = lists->count[0];
-  const int ngroups = (count + kGroup - 1) / kGroup;
+  const uint8_t* coarse_col = reinterpret_cast<const uint8_t*>(sm.pool) + j * 8;
+  const uint2* info_col = sm.pool + kCoarseUnits * kColumns + j;
   for (;;) {
-    int g = 0;
-    if (lane == 0) g = atomicAdd(&lists->next_group_rans, 1);
-    g = __shfl_sync(kFull, g, 0);
-    if (g >= ngroups) break;
-    const int first = g * kGroup;
-    const int gcount = min(kGroup, count - first);
-    // pool units of shard first + lane (lanes < gcount)
-    int need = 0;
-    if (lane < gcount) {
-      const RansTable& t = tables[first + lane];
-      need = t.valid ? kCoarseUnits + t.nsym : 0;
+    int p = 0;
+    if (my_l == 0) p = atomicAdd(&lists->next_group_rans, 1);
+    p = __shfl_sync(group, p, 4 * j);
+    if (p >= count) break;
+    const RansTable& t = tables[p];
+    if (!t.valid) continue;
+    const ShardInfo& si = shards[list_items[p]];
+    const FrameDesc& f = frames[si.frame];
+    const uint8_t* body = f.stream + si.offset;
+    uint32_t* out = folded + si.sample_base;
+    uint32_t x = t.state[my_l];
+    const int llen = t.lane_len[my_l];
+    const uint8_t* lb = body + t.lane_start[my_l];
+    const int nsym = t.nsym;
+    int cur = 0;
+    if (nsym <= kColumnSymbols) {
+      __syncwarp(group);  // the group's previous shard is decoded
+      for (int u = my_l; u < kCoarseUnits; u += 4)
+        sm.pool[u * kColumns + j] = make_uint2(t.coarse[2 * u], t.coarse[2 * u + 1]);
+      for (int i = my_l; i < nsym; i += 4) sm.pool[(kCoarseUnits + i) * kColumns + j] = t.info[i];
+      __syncwarp(group);
+      rans_decode_lane<3>(coarse_col, info_col, &sm.rings[0][lane], lb, llen, out, si.count, my_l, x, cur);
+    } else {
+      rans_decode_lane<0>(reinterpret_cast<const uint8_t*>(t.coarse), t.info, &sm.rings[0][lane], lb, llen, out,
+                          si.count, my_l, x, cur);
     }
-    for (int k = 0; k < gcount;) {
-      // the round: the longest run of shards k.. whose tables fit the pool
-      int inc = lane >= k && lane < gcount ? need : 0;
-#pragma unroll
-      for (int o = 1; o < kGroup; o <<= 1) {
-        const int v = __shfl_up_sync(kFull, inc, o);
-        if (lane >= o) inc += v;
-      }
-      const uint32_t fits = __ballot_sync(kFull, lane >= k && lane < gcount && inc <= kRansPoolUnits);
-      const int r = max(1, __popc(fits));  // one shard always fits (16 + 255 units)
-      if (lane < kGroup) sm.off[lane] = (lane >= k && lane < k + r && need > 0) ? inc - need : -1;
-      __syncwarp();
-      // tables of the round into the pool, coarse bucket tables
-      uint32_t* bitmap = &sm.rings[0][0];
-      for (int j = k; j < k + r; ++j) {
-        const int off = sm.off[j];
-        if (off < 0) continue;
-        const RansTable& t = tables[first + j];
-        const int n = t.nsym;
-        uint2* info = sm.pool + off + kCoarseUnits;
-        for (int i = lane; i < n; i += 32) info[i] = t.info[i];
-        for (int i = lane; i < 128; i += 32) bitmap[i] = 0;
-        __syncwarp();
-        for (int i = 1 + lane; i < n; i += 32) {
-          const uint32_t c = info[i].x & 0xffffu;
-          atomicOr(&bitmap[c >> 5], 1u << (c & 31));
-        }
-        __syncwarp();
-        // a bucket's first symbol is the number of symbol starts at or
-        // before its first slot; lane L covers bitmap words 4L..4L+3
-        uint32_t w[4];
-        int cnt = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          w[q] = bitmap[lane * 4 + q];
-          cnt += __popc(w[q]);
-        }
-        int sc = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int v = __shfl_up_sync(kFull, sc, o);
-          if (lane >= o) sc += v;
-        }
-        int base = sc - cnt;
-        constexpr int kPerWord = 32 >> kCoarseShift;  // buckets per bitmap word
-        uint32_t packed[kPerWord];                    // this lane's 4 * kPerWord bucket bytes
-#pragma unroll
-        for (int i = 0; i < kPerWord; ++i) packed[i] = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-#pragma unroll
-          for (int h = 0; h < kPerWord; ++h) {
-            const int byte = q * kPerWord + h;
-            const uint32_t upto = (2u << (h << kCoarseShift)) - 1u;  // bits 0 .. first slot of bucket h
-            packed[byte >> 2] |= static_cast<uint32_t>(base + __popc(w[q] & upto)) << (8 * (byte & 3));
-          }
-          base += __popc(w[q]);
-        }
-        uint32_t* cw = reinterpret_cast<uint32_t*>(sm.pool + off) + lane * kPerWord;
-#pragma unroll
-        for (int i = 0; i < kPerWord; ++i) cw[i] = packed[i];
-        __syncwarp();
-      }
-      // decode: lane 4j + l takes lane l of the round's j-th shard
-      const int j = k + my_g;
-      const int off = my_g < r ? sm.off[min(j, kGroup - 1)] : -1;
-      if (off >= 0) {
-        const int p = first + j;
-        const ShardInfo& si = shards[list_items[p]];
-        const FrameDesc& f = frames[si.frame];
-        const uint8_t* body = f.stream + si.offset;
-        uint32_t* out = folded + si.sample_base;
-        const int n = si.count;
-        const uint8_t* coarse = reinterpret_cast<const uint8_t*>(sm.pool + off);
-        const uint2* info = sm.pool + off + kCoarseUnits;
-        uint32_t x = tables[p].state[my_l];
-        const int llen = tables[p].lane_len[my_l];
-        const uint8_t* __restrict__ lb = body + tables[p].lane_start[my_l];
-        int cur = 0;
-        LaneRing ring;
-        ring.init(sm.rings[lane], lb, llen);
-        // Branch-free step: after x = freq*(x>>12) + slot - cum, x >= 2^11, so
-        // renormalisation shifts in one byte when x < 2^23 and a second when
-        // x < 2^15 (decode.cu:540-545), taken from the top of a four-byte
-        // window read ahead of the state chain; two steps use at most four
-        // bytes.  Reading past the lane is an error, found by the byte count.
-        auto step = [&](uint32_t& win, int idx) {
-          const uint32_t slot = x & ((1u << kRansTableLog) - 1u);
-          int sym = coarse[slot >> kCoarseShift];
-          uint2 e = info[sym];
-          while (slot >= (e.y & 0xffffu)) e = info[++sym];
-          out[idx] = e.y >> 16;
-          x = (e.x >> 16) * (x >> kRansTableLog) + slot - (e.x & 0xffffu);
-          const int nb = (x < kRansL) + (x < (kRansL >> 8));
-          x = __funnelshift_l(win, x, 8 * nb);
-          win <<= 8 * nb;
-          cur += nb;
-        };
-        int idx = my_l;
-        for (; idx + 4 < n; idx += 8) {
-          uint32_t win = ring.window(cur);
-          step(win, idx);
-          step(win, idx + 4);
-        }
-        if (idx < n) {
-          uint32_t win = ring.window(cur);
-          step(win, idx);
-        }
-        cp_async_wait<0>();
-        if (cur != llen || x != kRansL) set_status(&state[si.frame].status, 5);
-      }
-      __syncwarp();
-      k += r;
-    }
+    if (cur != llen || x != kRansL) set_status(&state[si.frame].status, 5);
   }
 }
 
