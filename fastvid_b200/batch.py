@@ -358,6 +358,141 @@ class BatchCodec:
         return out_planes
 
 
+    # ---- host buffers, pipelined ------------------------------------------
+    def encode_host(self, frames, *, chunk: int = 16, out: torch.Tensor | None = None, **params):
+        """Encode frames held in (preferably pinned) host memory; returns the
+        streams in pinned host memory: views of `out` (a pinned uint8 tensor
+        the caller allocates once and reuses -- pinning memory costs far more
+        than the copies) while it has room, else of new pinned buffers.
+
+        The batch runs in chunks of `chunk` frames: chunk i+2 is copied to the
+        device and chunk i-1's streams are copied back while chunk i is
+        encoded, on two copy streams beside the compute stream, so transfers
+        in both directions overlap the kernels.  Other arguments as encode();
+        per-frame lists are split with the frames.  Streams are identical to
+        encode()'s.
+        """
+        n = len(frames)
+        if n == 0:
+            return []
+        frames = [tuple(f) if not isinstance(f, torch.Tensor) else (f,) for f in frames]
+        per = {k: _per_frame(v, n, k) for k, v in params.items()}
+        with torch.cuda.device(self.device):
+            comp = torch.cuda.current_stream(self.device)
+            h2d, d2h = torch.cuda.Stream(self.device), torch.cuda.Stream(self.device)
+            h2d.wait_stream(comp)
+            d2h.wait_stream(comp)
+            bounds = list(range(0, n, chunk)) + [n]
+            staged: dict = {}
+
+            def stage(i):
+                lo, hi = bounds[i], bounds[i + 1]
+                with torch.cuda.stream(h2d):
+                    dev = [tuple(p.to(self.device, non_blocking=True) for p in f) for f in frames[lo:hi]]
+                    ev = torch.cuda.Event()
+                    ev.record(h2d)
+                staged[i] = (dev, ev)
+
+            res, cursor = [], 0
+            nchunks = len(bounds) - 1
+            for i in range(min(2, nchunks)):
+                stage(i)
+            for i in range(nchunks):
+                dev, ev = staged.pop(i)
+                comp.wait_event(ev)
+                for f in dev:
+                    for p in f:
+                        p.record_stream(comp)
+                lo, hi = bounds[i], bounds[i + 1]
+                streams = self.encode(dev, **{k: v[lo:hi] for k, v in per.items()})
+                if i + 2 < nchunks:
+                    stage(i + 2)
+                done = torch.cuda.Event()
+                done.record(comp)
+                total = sum(int(s.numel()) for s in streams)
+                if out is not None and cursor + total <= out.numel():
+                    host = out.narrow(0, cursor, total)
+                    cursor += total
+                else:
+                    host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+                arena = streams[0]._base if streams[0]._base is not None else streams[0]
+                with torch.cuda.stream(d2h):
+                    d2h.wait_event(done)
+                    arena.record_stream(d2h)
+                    host.copy_(arena.narrow(0, 0, total), non_blocking=True)
+                off = 0
+                for st in streams:
+                    res.append(host.narrow(0, off, st.numel()))
+                    off += st.numel()
+            d2h.synchronize()
+        return res
+
+    def decode_host(self, streams, *, chunk: int = 16, predictor: str = "wavefront",
+                    out: torch.Tensor | None = None):
+        """Decode streams held in (preferably pinned) host memory; returns
+        each frame's planes in pinned host memory -- views of `out` (a pinned
+        uint16 tensor reused across calls) while it has room -- pipelined
+        like encode_host (uploads of chunk i+2 and downloads of chunk i-1
+        overlap the decode of chunk i)."""
+        n = len(streams)
+        if n == 0:
+            return []
+        with torch.cuda.device(self.device):
+            comp = torch.cuda.current_stream(self.device)
+            h2d, d2h = torch.cuda.Stream(self.device), torch.cuda.Stream(self.device)
+            h2d.wait_stream(comp)
+            d2h.wait_stream(comp)
+            bounds = list(range(0, n, chunk)) + [n]
+            staged: dict = {}
+
+            def stage(i):
+                lo, hi = bounds[i], bounds[i + 1]
+                with torch.cuda.stream(h2d):
+                    dev = [s.to(self.device, non_blocking=True) for s in streams[lo:hi]]
+                    ev = torch.cuda.Event()
+                    ev.record(h2d)
+                heads = [bytes(s[:32].numpy().tobytes()) if (not s.is_cuda and s.numel() >= 32) else None
+                         for s in streams[lo:hi]]
+                staged[i] = (dev, ev, heads)
+
+            res, cursor = [], 0
+            nchunks = len(bounds) - 1
+            for i in range(min(2, nchunks)):
+                stage(i)
+            for i in range(nchunks):
+                dev, ev, heads = staged.pop(i)
+                comp.wait_event(ev)
+                for s in dev:
+                    s.record_stream(comp)
+                planes = self.decode(dev, predictor=predictor,
+                                     headers=heads if all(h is not None for h in heads) else None)
+                if i + 2 < nchunks:
+                    stage(i + 2)
+                done = torch.cuda.Event()
+                done.record(comp)
+                first = planes[0][0]
+                arena = first._base if first._base is not None else first
+                total = sum(p.numel() for f in planes for p in f)
+                if out is not None and cursor + total <= out.numel():
+                    host = out.narrow(0, cursor, total)
+                    cursor += total
+                else:
+                    host = torch.empty(total, dtype=torch.uint16, pin_memory=True)
+                with torch.cuda.stream(d2h):
+                    d2h.wait_event(done)
+                    arena.record_stream(d2h)
+                    host.copy_(arena.reshape(-1).narrow(0, 0, total), non_blocking=True)
+                off = 0
+                for f in planes:
+                    views = []
+                    for p in f:
+                        views.append(host.narrow(0, off, p.numel()).view(p.shape))
+                        off += p.numel()
+                    res.append(tuple(views))
+            d2h.synchronize()
+        return res
+
+
 _default: dict = {}
 
 

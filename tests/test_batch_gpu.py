@@ -118,3 +118,21 @@ def test_failing_frame_is_reported_at_its_own_index(cuda, mixed):
     streams = _encode(codec, [mixed[2], mixed[4], mixed[0], mixed[1]])
     for s, f in zip(streams, [mixed[2], mixed[4], mixed[0], mixed[1]]):
         assert bytes(s.cpu().numpy()) == f["oracle"]
+
+
+@pytest.mark.parametrize("chunk", [1, 3, 16])
+def test_host_pipelines_equal_the_device_path(cuda, mixed, chunk):
+    codec = BatchCodec("cuda")
+    host = [tuple(torch.from_numpy(p).pin_memory() for p in f["planes"]) for f in mixed]
+    params = dict(layout=[f["layout"] for f in mixed], bit_depth=[f["bit_depth"] for f in mixed],
+                  quality=[f["quality"] for f in mixed], tile_size=[f["tile"] for f in mixed])
+    streams = codec.encode_host(host, chunk=chunk, **params)
+    assert all(not s.is_cuda and s.is_pinned() for s in streams)
+    for f, s in zip(mixed, streams):
+        assert bytes(s.numpy()) == f["oracle"]
+    planes = codec.decode_host(streams, chunk=chunk)
+    for f, got in zip(mixed, planes):
+        want = oracle.decode(f["oracle"])
+        assert len(got) == len(want)
+        for g, w in zip(got, want):
+            assert not g.is_cuda and np.array_equal(g.numpy(), w)
