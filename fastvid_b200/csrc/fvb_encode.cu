@@ -1047,6 +1047,31 @@ __device__ __forceinline__ void put_byte(uint32_t* buf, int pos, uint32_t byte) 
   atomicOr(&buf[pos >> 2], (byte & 0xffu) << ((pos & 3) * 8));
 }
 
+// Record bytes [pos, pos+len) <- src[0, len) (global, any alignment), four
+// bytes per lane and step: record word d takes source bytes 4d-pos .. +3,
+// gathered from the two aligned source words that hold them (only words
+// holding a byte of the piece are read) and merged with one shared atomic,
+// the bytes outside the piece masked off.
+__device__ __forceinline__ void put_bytes(uint32_t* buf, int pos, const uint8_t* __restrict__ src, int len, int lane) {
+  if (len <= 0) return;
+  const uintptr_t sa = reinterpret_cast<uintptr_t>(src);
+  const uint32_t* __restrict__ sw = reinterpret_cast<const uint32_t*>(sa & ~static_cast<uintptr_t>(3));
+  const int h = static_cast<int>(sa & 3);
+  const int last_w = (h + len - 1) >> 2;  // last source word holding a piece byte
+  const int d1 = min((pos + len - 1) >> 2, kEmitWords - 1);
+  for (int d = (pos >> 2) + lane; d <= d1; d += 32) {
+    const int s0 = 4 * d - pos;  // piece offset of record byte 4d (>= -3)
+    const int q = h + s0;        // its byte index from sw (>= -3)
+    const int wi = q >> 2;       // floor: -1 for q in -3..-1
+    const uint32_t lo = wi >= 0 ? __ldg(sw + wi) : 0u;
+    const uint32_t hi = wi + 1 <= last_w ? __ldg(sw + wi + 1) : 0u;
+    const uint32_t v = __funnelshift_r(lo, hi, 8 * (q & 3));
+    const int k0 = max(0, -s0), k1 = min(3, len - 1 - s0);
+    const uint32_t mask = (0xffffffffu >> (8 * (3 - k1))) & (0xffffffffu << (8 * k0));
+    atomicOr(&buf[d], v & mask);
+  }
+}
+
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
 enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardInfo* __restrict__ shards,
                 int64_t total_shards, const uint32_t* __restrict__ folded,
@@ -1180,7 +1205,7 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
       const uint8_t* base = rans_scratch + s * static_cast<int64_t>(kRansScratchBytes);
       const uint8_t* ser = base + kRansTableWords * 4;
       const int tb = body - 28 - si.comp_lane[0] - si.comp_lane[1] - si.comp_lane[2] - si.comp_lane[3];
-      for (int i = lane; i < tb; i += 32) put_byte(buf, 3 + i, ser[i]);
+      put_bytes(buf, 3, ser, tb, lane);
       int pos = 3 + tb;
       if (lane < 3) {
         for (int b = 0; b < 4; ++b) put_byte(buf, pos + lane * 4 + b, static_cast<uint32_t>(si.comp_lane[lane]) >> (8 * b));
@@ -1193,7 +1218,7 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
       for (int l = 0; l < 4; ++l) {
         const int len = si.comp_lane[l];
         const uint8_t* lane_end = base + kRansTableWords * 4 + kRansSerialBytes + (l + 1) * kRansLaneBytes;
-        for (int i = lane; i < len; i += 32) put_byte(buf, pos + i, lane_end[i - len]);
+        put_bytes(buf, pos, lane_end - len, len, lane);
         pos += len;
       }
     }
