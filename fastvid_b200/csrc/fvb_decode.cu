@@ -819,8 +819,14 @@ __device__ void rec_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
     uint32_t pf[32];
     auto load_chunk = [&](int k) {
       const int col = k * 32 + lane;
+      const uint32_t* __restrict__ p = frows + col;
+      if (band_rows == 32 && col < W) {
 #pragma unroll
-      for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && col < W) ? __ldg(frows + static_cast<int64_t>(r) * W + col) : 0u;
+        for (int r = 0; r < 32; ++r) pf[r] = __ldg(p + static_cast<int64_t>(r) * W);
+      } else {
+#pragma unroll
+        for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && col < W) ? __ldg(p + static_cast<int64_t>(r) * W) : 0u;
+      }
     };
     auto store_chunk = [&](int k) {
       const int pj = k * 32 + lane;
@@ -830,8 +836,13 @@ __device__ void rec_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
     auto flush_chunk = [&](int k) {
       const int col = k * 32 + lane;
       if (col < W) {
-        for (int r = 0; r < band_rows; ++r)
-          orows[static_cast<int64_t>(r) * pitch + col] = sm.out[r * kSrcStride + ((col + r) & 63)];
+        uint16_t* __restrict__ q = orows + col;
+        if (band_rows == 32) {
+#pragma unroll
+          for (int r = 0; r < 32; ++r) q[static_cast<int64_t>(r) * pitch] = sm.out[r * kSrcStride + ((col + r) & 63)];
+        } else {
+          for (int r = 0; r < band_rows; ++r) q[static_cast<int64_t>(r) * pitch] = sm.out[r * kSrcStride + ((col + r) & 63)];
+        }
       }
     };
     load_chunk(0);

@@ -114,11 +114,16 @@ __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
     uint32_t pf[32];
     auto load_chunk = [&](int k) {
       const int col = k * 32 + lane;
+      const uint16_t* __restrict__ p = rows + col;
+      if (band_rows == 32 && col < W) {
 #pragma unroll
-      for (int r = 0; r < 32; ++r) {
-        pf[r] = (r < band_rows && col < W) ? rows[static_cast<int64_t>(r) * pitch + col] : 0u;
-        vmax = max(vmax, pf[r]);
+        for (int r = 0; r < 32; ++r) pf[r] = __ldg(p + static_cast<int64_t>(r) * pitch);
+      } else {
+#pragma unroll
+        for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && col < W) ? __ldg(p + static_cast<int64_t>(r) * pitch) : 0u;
       }
+#pragma unroll
+      for (int r = 0; r < 32; ++r) vmax = max(vmax, pf[r]);
     };
     auto store_chunk = [&](int k) {
       const int pj = k * 32 + lane;
@@ -128,8 +133,13 @@ __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
     auto flush_chunk = [&](int k) {
       const int col = k * 32 + lane;
       if (col < W) {
-        for (int r = 0; r < band_rows; ++r)
-          frows[static_cast<int64_t>(r) * W + col] = sm.fold[r * kFoldStride + ((col + r) & 63)];
+        uint32_t* __restrict__ q = frows + col;
+        if (band_rows == 32) {
+#pragma unroll
+          for (int r = 0; r < 32; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFoldStride + ((col + r) & 63)];
+        } else {
+          for (int r = 0; r < band_rows; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFoldStride + ((col + r) & 63)];
+        }
       }
     };
     load_chunk(0);
