@@ -781,7 +781,7 @@ __device__ __forceinline__ void rec_block(RecWarpSmem& sm, int lane, int t0, int
   const uint32_t* frow = sm.fold + lane * kFoldStride + (t0 & 32);
   uint16_t* orow = sm.out + lane * kSrcStride + (t0 & 32);
   uint16_t* crow = sm.carry + 32 - lane + t0;
-#pragma unroll
+#pragma unroll kBlockUnroll
   for (int u = 0; u < 32; ++u) {
     const uint32_t fv = frow[u];
     int32_t a = __shfl_up_sync(0xffffffffu, rec, 1);

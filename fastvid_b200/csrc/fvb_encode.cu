@@ -66,7 +66,7 @@ __device__ __forceinline__ void enc_block(EncWarpSmem& sm, int lane, int t0, int
   const uint16_t* srow = sm.src + lane * kSrcStride + (t0 & 32);
   uint32_t* frow = sm.fold + lane * kFoldStride + (t0 & 32);
   uint16_t* crow = sm.carry + 32 - lane + t0;  // carry index (t - lane) + 32
-#pragma unroll
+#pragma unroll kBlockUnroll
   for (int u = 0; u < 32; ++u) {
     const int32_t s = srow[u];
     int32_t a = __shfl_up_sync(0xffffffffu, rec, 1);

@@ -10,6 +10,10 @@ constexpr int kWarpsPerCta = 4;    // warps per CTA of the warp-per-item kernels
 constexpr int kSrcStride = 66;     // u16 ring row stride: 64 columns + 2 (33 words: conflict-free)
 constexpr int kFoldStride = 65;    // u32 ring row stride: 64 columns + 1 (conflict-free)
 constexpr int kFastMaxW = 512;     // widest tile of the register-wavefront path
+#ifndef FVB_BLOCK_UNROLL
+#define FVB_BLOCK_UNROLL 8
+#endif
+constexpr int kBlockUnroll = FVB_BLOCK_UNROLL;  // steps of a 32-step wavefront block unrolled
 
 // encoder
 __global__ void enc_init_kernel(const FrameDesc* frames, FrameState* state, int nframes);
