@@ -184,6 +184,7 @@ class Server:
         self._pending: collections.deque[Request] = collections.deque()
         self._cv = threading.Condition()
         self._closing = False
+        self._broken: BaseException | None = None
         self._resident = [0] * workers       # workspace bytes held per worker
         self._inflight = 0                   # output bytes of batches running
         self._running = 0                    # batches on the GPU
@@ -209,6 +210,8 @@ class Server:
         with self._cv:
             if self._closing:
                 raise RuntimeError("server is closed")
+            if self._broken is not None:
+                raise RuntimeError(f"serving worker failed: {self._broken!r}")
             self._pending.append(req)
             self._cv.notify_all()
         return req.future
@@ -269,6 +272,18 @@ class Server:
         return kind, chosen, out
 
     def _worker(self, w: int):
+        try:
+            self._serve(w)
+        except BaseException as exc:  # a worker that cannot go on fails what it would have answered
+            with self._cv:
+                self._broken = exc
+                pending, self._pending = list(self._pending), collections.deque()
+                self._cv.notify_all()
+            for r in pending:
+                if not r.future.done():
+                    r.future.set_exception(RuntimeError(f"serving worker failed: {exc!r}"))
+
+    def _serve(self, w: int):
         stream = self.backend.stream()
         self.backend.bind(stream)
         codec = self.backend.make_worker_codec()

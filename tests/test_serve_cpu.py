@@ -147,3 +147,19 @@ def test_open_loop_driver_reports_every_request():
     rep = report(recs, t0)
     assert rep["requests"] == 51 and rep["failed"] == 0
     assert 0 < rep["p50_ms"] <= rep["p99_ms"] <= rep["max_ms"]
+
+
+class BrokenBackend(FakeBackend):
+    def make_worker_codec(self):
+        raise RuntimeError("no device")
+
+
+def test_worker_failure_fails_requests_instead_of_hanging():
+    b = BrokenBackend()
+    s = Server(backend=b, workers=1)
+    b.server = s
+    for t in s._threads:
+        t.join(timeout=5)
+    with pytest.raises(RuntimeError, match="serving worker failed"):
+        s.submit_encode(1)
+    s.close()
