@@ -121,9 +121,12 @@ class BatchCodec:
         return self._ws_buf[:nbytes]
 
     # ---- encode -----------------------------------------------------------
-    def _encode_slot(self, frames_py: list[Frame]) -> _EncodeSlot:
-        key = tuple((f.layout, f.bit_depth, f.quality, f.width, f.height, f.tile_w, f.tile_h, f.fps_num, f.fps_den)
-                    for f in frames_py)
+    @staticmethod
+    def _enc_shape(f: Frame) -> tuple:
+        return (f.layout, f.bit_depth, f.quality, f.width, f.height, f.tile_w, f.tile_h, f.fps_num, f.fps_den)
+
+    def _encode_slot(self, frames_py: list[Frame], shapes: list | None = None) -> _EncodeSlot:
+        key = tuple(shapes) if shapes is not None else tuple(self._enc_shape(f) for f in frames_py)
         slot = self._enc.get(key)
         if slot is not None:
             return slot
@@ -158,31 +161,38 @@ class BatchCodec:
         qualities = _per_frame(quality, n, "quality")
         rates = _per_frame(frame_rate, n, "frame_rate")
         tiles = _per_frame(tile_size, n, "tile_size")
-        plans, ptrs, pitches = [], [], []
+        plans, shapes, ptrs, pitches = [], [], [], []
         for i, planes in enumerate(frames):
             lay = layouts[i]
             if lay is None:
                 lay = 0 if len(planes) == 1 else (1 if planes[1].shape[1] != planes[0].shape[1] else 2)
             elif isinstance(lay, str):
                 lay = _LAYOUTS_DEFAULT[lay]
+            # plan cache: the planes' shapes, strides, dtype and device index
+            # decide every check of plan_encode
             key = (lay, depths[i], qualities[i], tuple(rates[i]), tuple(tiles[i]),
-                   tuple((p.shape, p.dtype, p.device, p.stride()) for p in planes))
+                   tuple((p.shape, p.stride(), p.dtype, p.get_device()) for p in planes))
             hit = self._plans.get(key)
             if hit is not None:
-                frame, pit = hit
+                frame, pit, shape = hit
                 views = planes
             else:
                 frame, _, views, pit = plan_encode(list(planes), lay, depths[i], qualities[i], rates[i][0],
                                                    rates[i][1], tiles[i][0], tiles[i][1])
                 if views[0].device != self.device:
                     raise RuntimeError("all frames of a batch must be on the codec's device")
+                shape = self._enc_shape(frame)
                 if all(v is p for v, p in zip(views, planes)):  # no copy was needed: cacheable
-                    self._plans[key] = (frame, pit)
+                    self._plans[key] = (frame, pit, shape)
             plans.append(frame)
-            ptrs.extend([v.data_ptr() for v in views] + [0] * (3 - len(views)))
-            pitches.extend(list(pit) + [0] * (3 - len(pit)))
+            shapes.append(shape)
+            for v in views:
+                ptrs.append(v.data_ptr())
+            ptrs.extend((0,) * (3 - len(views)))
+            pitches.extend(pit)
+            pitches.extend((0,) * (3 - len(pit)))
         with torch.cuda.device(self.device):
-            slot = self._encode_slot(plans)
+            slot = self._encode_slot(plans, shapes)
             cur = torch.cuda.current_stream(self.device)
             p_arr = (ctypes.c_void_p * (3 * n))(*ptrs)
             q_arr = (ctypes.c_int64 * (3 * n))(*pitches)
@@ -233,9 +243,12 @@ class BatchCodec:
         return views
 
     # ---- decode -----------------------------------------------------------
-    def _decode_slot(self, frames_py: list[Frame], wavefront: bool) -> _DecodeSlot:
-        key = (wavefront,) + tuple((f.layout, f.bit_depth, f.quality, f.flags, f.width, f.height, f.tile_w, f.tile_h)
-                                   for f in frames_py)
+    @staticmethod
+    def _dec_shape(f: Frame) -> tuple:
+        return (f.layout, f.bit_depth, f.quality, f.flags, f.width, f.height, f.tile_w, f.tile_h)
+
+    def _decode_slot(self, frames_py: list[Frame], wavefront: bool, shapes: list | None = None) -> _DecodeSlot:
+        key = (wavefront,) + (tuple(shapes) if shapes is not None else tuple(self._dec_shape(f) for f in frames_py))
         slot = self._dec.get(key)
         if slot is not None:
             return slot
@@ -287,32 +300,36 @@ class BatchCodec:
                 _native.check(self.lib.fvb_gather_headers(s_arr, l_arr, n, self._hdr_scratch.data_ptr(),
                                                           self._hdr_scratch.numel(), heads, cur.cuda_stream))
                 raw = heads.raw
-            plans = []
+            plans, shapes, sizes = [], [], []
             for i, s in enumerate(dev_streams):
                 header = raw[32 * i:32 * i + 32]
                 key = (header, s.numel())
-                frame = self._dec_plans.get(key)
-                if frame is None:
+                hit = self._dec_plans.get(key)
+                if hit is None:
                     frame = plan_decode(s, header=header)[0]
-                    self._dec_plans[key] = frame
-                plans.append(frame)
-            slot = self._decode_slot(plans, predictor == "wavefront")
-            total = sum(f.samples for f in plans)
+                    cw = frame.plane_width[1] if frame.planes == 3 else 0
+                    # (frame, shape key, samples, planes, width, chroma width, luma and chroma samples)
+                    hit = (frame, self._dec_shape(frame), frame.samples, frame.planes, frame.width, cw,
+                           frame.width * frame.height, cw * frame.height)
+                    if len(self._dec_plans) < 65536:
+                        self._dec_plans[key] = hit
+                plans.append(hit)
+                shapes.append(hit[1])
+                sizes.append(hit[2])
+            slot = self._decode_slot([h[0] for h in plans], predictor == "wavefront", shapes)
+            total = sum(sizes)
             arena = torch.empty(total, dtype=torch.uint16, device=self.device)
             # plane pointers by arithmetic (Y, then Cb, then Cr of each frame);
             # the tensor views are made while the GPU decodes
             ptrs, pitches, off, base = [], [], 0, arena.data_ptr()
-            for f in plans:
-                y = f.width * f.height
-                if f.planes == 3:
-                    cw = f.plane_width[1]
-                    c = cw * f.height
-                    ptrs.extend([base + 2 * off, base + 2 * (off + y), base + 2 * (off + y + c)])
-                    pitches.extend([f.width, cw, cw])
+            for _, _, samples, planes_n, width, cw, y, c in plans:
+                if planes_n == 3:
+                    ptrs.extend((base + 2 * off, base + 2 * (off + y), base + 2 * (off + y + c)))
+                    pitches.extend((width, cw, cw))
                 else:
-                    ptrs.extend([base + 2 * off, 0, 0])
-                    pitches.extend([f.width, 0, 0])
-                off += f.samples
+                    ptrs.extend((base + 2 * off, 0, 0))
+                    pitches.extend((width, 0, 0))
+                off += samples
             p_arr = (ctypes.c_void_p * (3 * n))(*ptrs)
             q_arr = (ctypes.c_int64 * (3 * n))(*pitches)
             _native.check(self.lib.fvb_batch_decode_prepare(slot.frames, n, s_arr, l_arr, p_arr, q_arr,
@@ -320,9 +337,9 @@ class BatchCodec:
                                                             cur.cuda_stream))
             def views():
                 out, off = [], 0
-                for f in plans:
-                    out.append(tuple(plane_views(arena.narrow(0, off, f.samples), f)))
-                    off += f.samples
+                for f, _, samples, *_ in plans:
+                    out.append(tuple(plane_views(arena.narrow(0, off, samples), f)))
+                    off += samples
                 return out
 
             if self.use_graphs:
