@@ -830,7 +830,10 @@ enc_rans_kernel(const FrameState* __restrict__ state, ShardInfo* __restrict__ sh
     x += (e.y & 0x1fffu) + q * cmpl;
   };
   // symbols and table entries are loaded eight steps ahead of the state chain
-  constexpr int kAhead = 8;
+#ifndef FVB_RANS_AHEAD
+#define FVB_RANS_AHEAD 16
+#endif
+  constexpr int kAhead = FVB_RANS_AHEAD;
   int c = 0;
   for (; c + kAhead <= steps; c += kAhead) {
     uint32_t v[kAhead];
