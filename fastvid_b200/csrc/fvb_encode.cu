@@ -343,7 +343,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
   // value sit 520 words apart, in different banks.  list: the present values
   // in increasing order, value | total count << 16.  ring: each lane's next
   // kRing 16-byte pieces of the warp's block stream.
-  constexpr int kRing = 6;
+  constexpr int kRing = 6;  // measured on the 96-frame mix: 6 pieces ahead beats 8
   __shared__ __align__(16) uint32_t hcls_all[kWarpsPerCta][2][520];
   __shared__ uint32_t list_all[kWarpsPerCta][512];
   __shared__ __align__(16) uint4 ring_all[kWarpsPerCta][kRing * 32];
@@ -830,10 +830,7 @@ enc_rans_kernel(const FrameState* __restrict__ state, ShardInfo* __restrict__ sh
     x += (e.y & 0x1fffu) + q * cmpl;
   };
   // symbols and table entries are loaded eight steps ahead of the state chain
-#ifndef FVB_RANS_AHEAD
-#define FVB_RANS_AHEAD 16
-#endif
-  constexpr int kAhead = FVB_RANS_AHEAD;
+  constexpr int kAhead = 16;  // measured on the 96-frame mix: 16 beats 4, 8 and 32
   int c = 0;
   for (; c + kAhead <= steps; c += kAhead) {
     uint32_t v[kAhead];
