@@ -159,6 +159,15 @@ class CodecBackend:
         torch.cuda.current_stream(self.device).synchronize()  # answers are complete when delivered
         return out
 
+    def warm(self, nbytes: int):
+        """Allocate and free `nbytes` on the calling worker's stream, so the
+        caching allocator serves that worker's later outputs from cached
+        memory: growing the pool mid-run (cudaMalloc) stalled single batches
+        for tens of milliseconds."""
+        if nbytes > 0:
+            block = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            del block
+
     def stream(self):
         return torch.cuda.Stream(self.device)
 
@@ -176,9 +185,14 @@ class Server:
     """
 
     def __init__(self, device=None, *, memory_budget: int = 40 << 30, workers: int = 3,
-                 max_batch_frames: int = 64, max_batch_pixels: int = 200_000_000, backend=None):
+                 max_batch_frames: int = 64, max_batch_pixels: int = 200_000_000, backend=None,
+                 warm_bytes: int | None = None):
+        """warm_bytes: device memory each worker allocates and frees once at
+        start on its own stream (default: an eighth of the budget per
+        worker, at most 2 GiB), so outputs come from the allocator's cache."""
         self.backend = backend if backend is not None else CodecBackend(device if device is not None else "cuda")
         self.budget = int(memory_budget)
+        self.warm_bytes = (min(2 << 30, self.budget // (8 * workers)) if warm_bytes is None else int(warm_bytes))
         self.max_frames = max_batch_frames
         self.max_pixels = max_batch_pixels
         self._pending: collections.deque[Request] = collections.deque()
@@ -286,6 +300,8 @@ class Server:
     def _serve(self, w: int):
         stream = self.backend.stream()
         self.backend.bind(stream)
+        if hasattr(self.backend, "warm"):
+            self.backend.warm(self.warm_bytes)
         codec = self.backend.make_worker_codec()
         while True:
             release = False
@@ -404,9 +420,23 @@ def run_open_loop(server: Server, items, rate: float | None, seed: int = 0, keep
             if remaining[0] == 0:
                 all_done.set()
 
+    def copy(answer):
+        # an answer is a view of its batch's output arena; a copy lets the
+        # arena go back to the allocator
+        if isinstance(answer, torch.Tensor):
+            return answer.clone()
+        if isinstance(answer, tuple):
+            return tuple(copy(a) for a in answer)
+        return answer
+
+    def keeper(i):
+        def done(f):
+            if f.exception() is None:
+                kept[i] = copy(f.result())
+        return done
+
     t0 = time.perf_counter()
     t = t0
-    pending = []
     for i, (kind, payload, params) in enumerate(items):
         if rate:
             t += rng.expovariate(rate)
@@ -416,13 +446,11 @@ def run_open_loop(server: Server, items, rate: float | None, seed: int = 0, keep
         fut = server.submit_encode(payload, **params) if kind == "encode" else server.submit_decode(payload, **params)
         rids.append(fut.rid)
         if i in keep:
-            pending.append((i, fut))
-        fut.add_done_callback(answered)  # other answers are released with their futures
+            fut.add_done_callback(keeper(i))
+        fut.add_done_callback(answered)  # answers are released with their futures
     if items:
         all_done.wait()
     want = set(rids)
     with server._cv:
         got = {r.rid: r for r in server.completed if r.rid in want}
-    for i, fut in pending:
-        kept[i] = fut.result()
     return [got[r] for r in rids], t0, kept
