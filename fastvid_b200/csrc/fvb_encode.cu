@@ -829,7 +829,7 @@ enc_rans_kernel(const FrameState* __restrict__ state, ShardInfo* __restrict__ sh
     const uint32_t q = __umulhi(x, e.x) >> (e.y >> 25);
     x += (e.y & 0x1fffu) + q * cmpl;
   };
-  // symbols and table entries are loaded eight steps ahead of the state chain
+  // symbols and table entries are loaded kAhead steps ahead of the state chain
   constexpr int kAhead = 16;  // measured on the 96-frame mix: 16 beats 4, 8 and 32
   int c = 0;
   for (; c + kAhead <= steps; c += kAhead) {
