@@ -138,26 +138,28 @@ __global__ void dec_parse_kernel(const FrameDesc* __restrict__ frames, FrameStat
 // Entropy decode (decode.cu:222-550).  dec_parse bins shards by mode; then
 //   dec_rans_tables  one thread per rANS shard parses its order-0 table
 //                    serially (decode.cu:456-517) into a table record
-//   dec_rans         a warp takes eight rANS shards: copies their tables into
-//                    shared memory, builds a coarse slot table, and lane 4g+l
-//                    decodes lane l of shard g (decode.cu:530-549)
+//   dec_rans         a 4-lane group streams rANS shards: it copies a shard's
+//                    table into shared memory, builds a bucket table of
+//                    symbol starts, and lane l decodes lane l of the shard
+//                    (decode.cu:530-549)
 //   dec_other        a warp takes eight Rice, zero-run or block shards: Rice
 //                    lane l of shard g on lane 4g+l (decode.cu:297-340),
 //                    zero-run shard g on lane 4g (decode.cu:237-295), block
 //                    shards one after another warp-wide (decode.cu:342-396)
 
-// Measured on the 48-frame mix: 32-slot buckets beat 8- and 16-slot buckets
-// and a one-ahead symbol lookup.
-constexpr int kGroup = 8;        // shards per warp
-constexpr int kCoarseShift = 5;  // coarse bucket = 32 slots
+constexpr int kGroup = 8;         // shards per warp
+constexpr int kBucketShift = 4;   // a bucket covers 16 slots
+constexpr int kBuckets = (1 << kRansTableLog) >> kBucketShift;
 
+// One parsed order-0 table (decode.cu:456-517).  Symbol i covers slots
+// cum_i .. cum_i + freq_i - 1 of the 4096-slot ring.
 struct RansTable {
   int32_t lane_start[4], lane_len[4];
   uint32_t state[4];
   int32_t nsym, valid;
   int32_t pad[2];
-  uint32_t coarse[32];  // first symbol of each 32-slot bucket, one byte per bucket
-  uint2 info[256];  // x: cum | freq << 16, y: (cum + freq) | value << 16 (value as u16, decode.cu:484)
+  uint32_t freqcum[256];  // cum | freq << 12 (freq up to 4096: 13 bits)
+  uint32_t value[256];    // the symbol's value as u16 (decode.cu:484)
 };
 
 size_t dec_rans_table_bytes() { return sizeof(RansTable); }
@@ -321,7 +323,8 @@ __device__ bool rans_parse_serial(const uint8_t* __restrict__ body, int64_t blen
     if (fr == 0 || fr > (1u << kRansTableLog) - assigned ||
         (i + 1 != n && fr == (1u << kRansTableLog) - assigned))
       return false;
-    t.info[i] = make_uint2(assigned | (fr << 16), (assigned + fr) | ((value & 0xffffu) << 16));
+    t.freqcum[i] = assigned | (fr << 12);
+    t.value[i] = value & 0xffffu;
     assigned += fr;
     prev = value;
   }
@@ -375,54 +378,64 @@ dec_rans_tables_kernel(const FrameDesc* __restrict__ frames, FrameState* __restr
       const FrameDesc& f = frames[si.frame];
       ok = rans_parse_serial(f.stream + si.offset, si.body, static_cast<uint32_t>(f.max_sample) * 2u, t);
       if (!ok) set_status(&st.status, 5);
-      if (ok) {
-        // bucket b (slots 32b..32b+31) starts in the last symbol whose
-        // cumulative start is at or before slot 32b
-        const int n = t.nsym;
-        int sym = 0;
-        for (int w = 0; w < 32; ++w) {
-          uint32_t packed = 0;
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const uint32_t first_slot = static_cast<uint32_t>(w * 4 + q) << kCoarseShift;
-            while (sym + 1 < n && (t.info[sym + 1].x & 0xffffu) <= first_slot) ++sym;
-            packed |= static_cast<uint32_t>(sym) << (8 * q);
-          }
-          t.coarse[w] = packed;
-        }
-      }
     }
     t.valid = ok;
   }
 }
 
-// Shared memory of one dec_rans warp: the eight 4-lane groups' tables,
-// interleaved -- unit u (8 bytes) of group j at pool[u * 8 + j], so lookups
-// of different groups fall in different banks -- and the lanes' byte rings.
-// A group's column holds its shard's 128-entry coarse table (16 units) and up
-// to 40 info entries: the handful of symbols a predicted shard holds.
-// Shards with more symbols are decoded from their table in global memory.
-constexpr int kColumns = 8;                    // 4-lane groups per warp
-constexpr int kColumnUnits = 56;               // 16 coarse + 40 info
-constexpr int kCoarseUnits = (1 << kRansTableLog) >> kCoarseShift >> 3;
-constexpr int kColumnSymbols = kColumnUnits - kCoarseUnits;
+// Shared memory of one dec_rans warp: one column per 4-lane group, the
+// columns interleaved word by word (word k of group j at pool[k * 8 + j]) so
+// that the groups' lookups fall in different banks; and the lanes' byte
+// rings.  A column holds the shard's bucket table and, for tables of up to
+// 64 symbols (a predicted shard holds a few dozen), its freq|cum and value
+// words; larger tables are read from global memory.
+constexpr int kColumns = 8;  // 4-lane groups per warp
+constexpr int kColumnSymbols = 64;
+constexpr int kColumnWords = kBuckets + 2 * kColumnSymbols;
 
 struct RansWarpSm {
-  uint2 pool[kColumns * kColumnUnits];
+  uint32_t pool[kColumns * kColumnWords];
   // per-lane byte rings, slot-major: rings[s][lane]
   uint32_t rings[LaneRing::kWords][32];
 };
 
 size_t dec_rans_smem() { return sizeof(RansWarpSm) * kWarpsPerCta; }
 
+// Bucket table of one shard: word u = (symbol holding slot 16u) << 16, with
+// bit i set for every symbol whose range starts at slot 16u + i (i = 1..15).
+// The symbol holding slot s is then the bucket's first symbol plus the
+// starts at or below s inside the bucket -- one shared load and a population
+// count, no search.  `fc` is the freq|cum list at a stride of 2^fc_shift
+// words; lane l of the group writes buckets 64l .. 64l + 63.
+__device__ __forceinline__ void build_buckets(uint32_t* bcol, const uint32_t* fc, int fc_shift, int nsym,
+                                              int my_l) {
+  constexpr uint32_t kSlots = 1u << kRansTableLog;
+  auto start = [&](int i) { return i < nsym ? (fc[i << fc_shift] & (kSlots - 1u)) : kSlots; };
+  int s = 0;
+  uint32_t next = start(1);  // first slot of symbol s + 1
+  for (int k = 0; k < kBuckets / 4; ++k) {
+    const uint32_t u = static_cast<uint32_t>(my_l * (kBuckets / 4) + k);
+    const uint32_t lo = u << kBucketShift;
+    while (next <= lo) next = start(++s + 1);
+    uint32_t w = static_cast<uint32_t>(s) << 16;
+    for (int i = s + 1; next < lo + (1u << kBucketShift);) {
+      w |= 1u << (next - lo);
+      next = start(++i);
+    }
+    next = start(s + 1);
+    bcol[u * kColumns] = w;
+  }
+}
+
 // Decode lane `my_l` of one shard: n symbols, this lane's byte range `lb`
-// (llen bytes), initial state x; the shard's coarse table and info entries
-// at a stride of 2^LOG_S units.  Returns the bytes consumed and the final
-// state.
+// (llen bytes), initial state x; the bucket table at a stride of 8 words,
+// the freq|cum and value words at a stride of 2^LOG_S.  Returns the bytes
+// consumed and the final state.
 template <int LOG_S>
-__device__ __forceinline__ void rans_decode_lane(const uint8_t* __restrict__ coarse_col, const uint2* __restrict__ info_col,
-                                                 uint32_t* ring_smem, const uint8_t* __restrict__ lb, int llen,
-                                                 uint32_t* __restrict__ out, int n, int my_l, uint32_t& x, int& cur) {
+__device__ __forceinline__ void rans_decode_lane(const uint32_t* __restrict__ bcol, const uint32_t* __restrict__ fc_col,
+                                                 const uint32_t* __restrict__ val_col, uint32_t* ring_smem,
+                                                 const uint8_t* __restrict__ lb, int llen, uint32_t* __restrict__ out,
+                                                 int n, int my_l, uint32_t& x, int& cur) {
   LaneRing ring;
   ring.init(ring_smem, lb, llen);
   cur = 0;
@@ -433,12 +446,12 @@ __device__ __forceinline__ void rans_decode_lane(const uint8_t* __restrict__ coa
   // Reading past the lane is an error, found by the byte count.
   auto step = [&](uint32_t& win, int idx) {
     const uint32_t slot = x & ((1u << kRansTableLog) - 1u);
-    const uint32_t b = slot >> kCoarseShift;
-    int sym = coarse_col[((b >> 3) << (LOG_S + 3)) + (b & 7)];
-    uint2 e = info_col[sym << LOG_S];
-    while (slot >= (e.y & 0xffffu)) e = info_col[(++sym) << LOG_S];
-    out[idx] = e.y >> 16;
-    x = (e.x >> 16) * (x >> kRansTableLog) + slot - (e.x & 0xffffu);
+    const uint32_t bw = bcol[(slot >> kBucketShift) * kColumns];
+    // starts at offsets 1..r of the bucket survive the shift by 31 - r
+    const uint32_t sym = (bw >> 16) + __popc(bw << ((slot & ((1u << kBucketShift) - 1u)) ^ 31u));
+    const uint32_t fc = fc_col[sym << LOG_S];
+    out[idx] = val_col[sym << LOG_S];
+    x = (fc >> 12) * (x >> kRansTableLog) + slot - (fc & ((1u << kRansTableLog) - 1u));
     const int nb = (x < kRansL) + (x < (kRansL >> 8));
     x = __funnelshift_l(win, x, 8 * nb);
     win <<= 8 * nb;
@@ -458,9 +471,9 @@ __device__ __forceinline__ void rans_decode_lane(const uint8_t* __restrict__ coa
 }
 
 // Each 4-lane group streams rANS shards: it claims the next shard from the
-// list, copies the shard's tables into its column and decodes its four
-// lanes, then claims another -- so every lane stays busy until the list is
-// done, whatever the mix of shards.
+// list, builds the shard's tables in its column and decodes its four lanes,
+// then claims another -- so every lane stays busy until the list is done,
+// whatever the mix of shards.
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
 dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
                 const ShardInfo* __restrict__ shards, DecodeLists* __restrict__ lists,
@@ -472,8 +485,9 @@ dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
   const int j = lane >> 2, my_l = lane & 3;
   const unsigned group = 0xfu << (4 * j);
   const int count = lists->count[0];
-  const uint8_t* coarse_col = reinterpret_cast<const uint8_t*>(sm.pool) + j * 8;
-  const uint2* info_col = sm.pool + kCoarseUnits * kColumns + j;
+  uint32_t* bcol = sm.pool + j;
+  uint32_t* fc_col = sm.pool + kBuckets * kColumns + j;
+  uint32_t* val_col = sm.pool + (kBuckets + kColumnSymbols) * kColumns + j;
   for (;;) {
     int p = 0;
     if (my_l == 0) p = atomicAdd(&lists->next_group_rans, 1);
@@ -489,18 +503,24 @@ dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
     const int llen = t.lane_len[my_l];
     const uint8_t* lb = body + t.lane_start[my_l];
     const int nsym = t.nsym;
+    const bool local = nsym <= kColumnSymbols;
     int cur = 0;
-    if (nsym <= kColumnSymbols) {
-      __syncwarp(group);  // the group's previous shard is decoded
-      for (int u = my_l; u < kCoarseUnits; u += 4)
-        sm.pool[u * kColumns + j] = make_uint2(t.coarse[2 * u], t.coarse[2 * u + 1]);
-      for (int i = my_l; i < nsym; i += 4) sm.pool[(kCoarseUnits + i) * kColumns + j] = t.info[i];
+    __syncwarp(group);  // the group's previous shard is decoded
+    if (local) {
+      for (int i = my_l; i < nsym; i += 4) {
+        fc_col[i * kColumns] = t.freqcum[i];
+        val_col[i * kColumns] = t.value[i];
+      }
       __syncwarp(group);
-      rans_decode_lane<3>(coarse_col, info_col, &sm.rings[0][lane], lb, llen, out, si.count, my_l, x, cur);
+      build_buckets(bcol, fc_col, 3, nsym, my_l);
     } else {
-      rans_decode_lane<0>(reinterpret_cast<const uint8_t*>(t.coarse), t.info, &sm.rings[0][lane], lb, llen, out,
-                          si.count, my_l, x, cur);
+      build_buckets(bcol, t.freqcum, 0, nsym, my_l);
     }
+    __syncwarp(group);
+    if (local)
+      rans_decode_lane<3>(bcol, fc_col, val_col, &sm.rings[0][lane], lb, llen, out, si.count, my_l, x, cur);
+    else
+      rans_decode_lane<0>(bcol, t.freqcum, t.value, &sm.rings[0][lane], lb, llen, out, si.count, my_l, x, cur);
     if (cur != llen || x != kRansL) set_status(&state[si.frame].status, 5);
   }
 }
