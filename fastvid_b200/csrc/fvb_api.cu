@@ -238,6 +238,36 @@ int device_sms() {
   return sms[dev];
 }
 
+// A side stream with fork/join events, one per host thread and device.
+// dec_other (Rice, zero-run and block shards) depends on dec_parse only, so
+// on large batches it runs on the side stream beside dec_rans and fills the
+// threads and issue slots that the rANS decoder leaves free on every SM.
+// Per thread, so concurrent callers never share an event.
+struct SideStream {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+int side_stream(SideStream** out) {
+  thread_local SideStream per_device[64];
+  *out = nullptr;
+  int dev = 0;
+  FVB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return FVB_OK;
+  SideStream& ss = per_device[dev];
+  if (!ss.stream) {
+    FVB_CUDA(cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming));
+    FVB_CUDA(cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming));
+    FVB_CUDA(cudaStreamCreateWithFlags(&ss.stream, cudaStreamNonBlocking));
+  }
+  *out = &ss;
+  return FVB_OK;
+}
+
+// batches of at least this many shards (about 4 million samples) decode
+// their non-rANS shards on the side stream
+constexpr int64_t kSideStreamShards = 1024;
+
 int ensure_smem_attrs() {
   static bool done[64] = {false};
   int dev = 0;
@@ -867,6 +897,12 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
                                                                            tables);
   }
   FVB_LAUNCHED("dec_rans_tables_kernel");
+  SideStream* side = nullptr;
+  if (t.shards >= kSideStreamShards) {
+    rc = side_stream(&side);
+    if (rc) return rc;
+  }
+  if (side) FVB_CUDA(cudaEventRecord(side->fork, stream));
   {
     LaunchScope scope_(K_DEC_RANS, stream);
     dec_rans_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), kWarpsPerCta, ctas(K_DEC_RANS)), kWarpsPerCta * 32, dec_rans_smem(),
@@ -875,11 +911,20 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
   }
   FVB_LAUNCHED("dec_rans_kernel");
   {
-    LaunchScope scope_(K_DEC_OTHER, stream);
-    dec_other_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), 4, ctas(K_DEC_OTHER)), 128, 0, stream>>>(
-        frames_d, state, shards, t.shards, lists, items, folded);
+    // launched after dec_rans, so the rANS decoder's CTAs are placed first
+    cudaStream_t other = side ? side->stream : stream;
+    if (side) FVB_CUDA(cudaStreamWaitEvent(other, side->fork, 0));
+    {
+      LaunchScope scope_(K_DEC_OTHER, other);
+      dec_other_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), 4, ctas(K_DEC_OTHER)), 128, 0, other>>>(
+          frames_d, state, shards, t.shards, lists, items, folded);
+    }
+    FVB_LAUNCHED("dec_other_kernel");
+    if (side) {
+      FVB_CUDA(cudaEventRecord(side->join, other));
+      FVB_CUDA(cudaStreamWaitEvent(stream, side->join, 0));
+    }
   }
-  FVB_LAUNCHED("dec_other_kernel");
   if (wavefront) {
     {
       LaunchScope scope_(K_DEC_RECON, stream);
