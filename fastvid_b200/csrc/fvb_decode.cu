@@ -232,30 +232,36 @@ struct ByteWindow {
 };
 
 
-// A lane's byte stream through a private ring of 16 words in shared memory,
-// fed by cp.async four words at a time and kept at least 12 words ahead of
-// the read position: reads are shared-memory loads whose data arrived long
-// before.  Word w of the aligned range lives in slot w % 16; slot s of lane l
-// is word s * 32 + l of the warp's ring block, so every lane reads and fills
-// its own bank whatever its position.  Only words holding a byte of the lane
-// are copied (others keep stale bytes, and reading them is an overrun that
-// the byte count check reports).
+// A lane's byte stream through a private ring of 32 words in shared memory,
+// fed by cp.async: 24 words before the first read, then two words with every
+// eight-byte read -- as many as four decoding steps can consume -- so the
+// ring stays at least 24 words ahead of the read position, and a read, which
+// may leave the newest four copy groups in flight, only touches words copied
+// long before.  There is no refill branch: every read issues its two copies
+// under predicates.  Word w of the aligned range lives in slot w % 32; slot s
+// of lane l is word s * 32 + l of the warp's ring block, so every lane reads
+// and fills its own bank whatever its position.  Only words holding a byte of
+// the lane are copied (others keep stale bytes, and reading them is an
+// overrun that the byte count check reports).
 struct LaneRing {
-  static constexpr int kWords = 16;
+  static constexpr int kWords = 32;    // slots per lane
+  static constexpr int kFill = 24;     // words copied before the first read
+  static constexpr int kInFlight = 4;  // copy groups a read may leave pending
   uint32_t* ring;          // slot 0 of this lane (slots 32 words apart)
   const uint32_t* words;   // aligned base of the lane's bytes
   int head;                // lane byte 0 = byte `head` of word 0
   int last;                // last word holding a lane byte (-1: none)
-  int fetched;             // words issued so far (multiple of 4)
+  int fetched;             // next word to copy
 
-  __device__ void fetch() {
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int w = fetched + j;
-      if (w <= last) cp_async4(ring + (w & (kWords - 1)) * 32, words + w);
-    }
-    cp_async_commit();
-    fetched += 4;
+  // Copy word w into its slot if it holds a lane byte and its slot is free
+  // (the word 32 below it is behind the read position `low`).
+  __device__ void issue(int w, int low) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(ring + (w & (kWords - 1)) * 32));
+    const int ok = (w <= last) & (w <= low + kWords - 1);
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %2, 0;\n @p cp.async.ca.shared.global [%0], [%1], 4;\n}\n" ::"r"(s),
+        "l"(words + w), "r"(ok)
+        : "memory");
   }
   __device__ void init(uint32_t* ring_smem, const uint8_t* p, int len) {
     const uintptr_t a = reinterpret_cast<uintptr_t>(p);
@@ -263,22 +269,30 @@ struct LaneRing {
     words = reinterpret_cast<const uint32_t*>(a - head);
     ring = ring_smem;
     last = len > 0 ? (head + len - 1) >> 2 : -1;
-    fetched = 0;
-    fetch();
-    fetch();
-    fetch();
+#pragma unroll
+    for (int i = 0; i < kFill; ++i) issue(i, 0);
+    fetched = kFill;
+    cp_async_commit();
   }
-  // The four bytes at lane positions cur..cur+3, first byte in the top bits;
-  // cur advances by at most four between calls.  After a fetch the ring
-  // holds words w .. w+11 or more; all but the newest group are complete,
-  // which covers words w and w + 1.
-  __device__ uint32_t window(int cur) {
+  __device__ void ready() { cp_async_wait<0>(); }
+  // The eight bytes at lane positions cur..cur+7, first byte in the top
+  // bits; cur advances by at most eight between calls.
+  __device__ uint64_t window(int cur) {
     const int pos = head + cur;
     const int w = pos >> 2;
-    if (fetched - w < 12) fetch();
-    cp_async_wait<1>();  // the newest group may stay in flight
-    const uint32_t lo = ring[(w & (kWords - 1)) * 32], hi = ring[((w + 1) & (kWords - 1)) * 32];
-    return __byte_perm(__funnelshift_r(lo, hi, 8 * (pos & 3)), 0, 0x0123);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      issue(fetched, w);
+      fetched += fetched <= w + kWords - 1;
+    }
+    cp_async_commit();
+    cp_async_wait<kInFlight>();
+    const uint32_t a = ring[(w & (kWords - 1)) * 32], b = ring[((w + 1) & (kWords - 1)) * 32],
+                   c = ring[((w + 2) & (kWords - 1)) * 32];
+    const int sh = 8 * (pos & 3);
+    const uint32_t hi = __byte_perm(__funnelshift_r(a, b, sh), 0, 0x0123);
+    const uint32_t lo = __byte_perm(__funnelshift_r(b, c, sh), 0, 0x0123);
+    return (static_cast<uint64_t>(hi) << 32) | lo;
   }
 };
 
@@ -427,24 +441,22 @@ __device__ __forceinline__ void build_buckets(uint32_t* bcol, const uint32_t* fc
   }
 }
 
-// Decode lane `my_l` of one shard: n symbols, this lane's byte range `lb`
-// (llen bytes), initial state x; the bucket table at a stride of 8 words,
+// Decode lane `my_l` of one shard: n symbols from this lane's byte ring,
+// initial state x; the bucket table at a stride of 8 words,
 // the freq|cum and value words at a stride of 2^LOG_S.  Returns the bytes
 // consumed and the final state.
 template <int LOG_S>
 __device__ __forceinline__ void rans_decode_lane(const uint32_t* __restrict__ bcol, const uint32_t* __restrict__ fc_col,
-                                                 const uint32_t* __restrict__ val_col, uint32_t* ring_smem,
-                                                 const uint8_t* __restrict__ lb, int llen, uint32_t* __restrict__ out,
-                                                 int n, int my_l, uint32_t& x, int& cur) {
-  LaneRing ring;
-  ring.init(ring_smem, lb, llen);
+                                                 const uint32_t* __restrict__ val_col, LaneRing& ring,
+                                                 uint32_t* __restrict__ out, int n, int my_l, uint32_t& x, int& cur) {
   cur = 0;
+  ring.ready();
   // Branch-free step: after x = freq*(x>>12) + slot - cum, x >= 2^11, so
   // renormalisation shifts in one byte when x < 2^23 and a second when
-  // x < 2^15 (decode.cu:540-545), taken from the top of a four-byte window
-  // read ahead of the state chain; two steps use at most four bytes.
+  // x < 2^15 (decode.cu:540-545), taken from the top of an eight-byte window
+  // read ahead of the state chain; four steps use at most eight bytes.
   // Reading past the lane is an error, found by the byte count.
-  auto step = [&](uint32_t& win, int idx) {
+  auto step = [&](uint64_t& win, int idx) {
     const uint32_t slot = x & ((1u << kRansTableLog) - 1u);
     const uint32_t bw = bcol[(slot >> kBucketShift) * kColumns];
     // starts at offsets 1..r of the bucket survive the shift by 31 - r
@@ -453,19 +465,21 @@ __device__ __forceinline__ void rans_decode_lane(const uint32_t* __restrict__ bc
     out[idx] = val_col[sym << LOG_S];
     x = (fc >> 12) * (x >> kRansTableLog) + slot - (fc & ((1u << kRansTableLog) - 1u));
     const int nb = (x < kRansL) + (x < (kRansL >> 8));
-    x = __funnelshift_l(win, x, 8 * nb);
+    x = __funnelshift_l(static_cast<uint32_t>(win >> 32), x, 8 * nb);
     win <<= 8 * nb;
     cur += nb;
   };
   int idx = my_l;
-  for (; idx + 4 < n; idx += 8) {
-    uint32_t win = ring.window(cur);
+  for (; idx + 12 < n; idx += 16) {
+    uint64_t win = ring.window(cur);
     step(win, idx);
     step(win, idx + 4);
+    step(win, idx + 8);
+    step(win, idx + 12);
   }
   if (idx < n) {
-    uint32_t win = ring.window(cur);
-    step(win, idx);
+    uint64_t win = ring.window(cur);
+    for (; idx < n; idx += 4) step(win, idx);  // at most three steps
   }
   cp_async_wait<0>();
 }
@@ -505,6 +519,8 @@ dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
     const int nsym = t.nsym;
     const bool local = nsym <= kColumnSymbols;
     int cur = 0;
+    LaneRing ring;
+    ring.init(&sm.rings[0][lane], lb, llen);  // the first copies land while the tables are built
     __syncwarp(group);  // the group's previous shard is decoded
     if (local) {
       for (int i = my_l; i < nsym; i += 4) {
@@ -518,9 +534,9 @@ dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
     }
     __syncwarp(group);
     if (local)
-      rans_decode_lane<3>(bcol, fc_col, val_col, &sm.rings[0][lane], lb, llen, out, si.count, my_l, x, cur);
+      rans_decode_lane<3>(bcol, fc_col, val_col, ring, out, si.count, my_l, x, cur);
     else
-      rans_decode_lane<0>(bcol, t.freqcum, t.value, &sm.rings[0][lane], lb, llen, out, si.count, my_l, x, cur);
+      rans_decode_lane<0>(bcol, t.freqcum, t.value, ring, out, si.count, my_l, x, cur);
     if (cur != llen || x != kRansL) set_status(&state[si.frame].status, 5);
   }
 }
