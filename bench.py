@@ -345,24 +345,13 @@ def main():
     device = torch.device("cuda", local_rank)
     if table:
         autotune.apply(table)
-    dist = None
-    if world > 1:
-        import datetime
+    # replicas: one process per GPU; the process group carries only the
+    # barrier around timed regions and the max over ranks
+    from fastvid_b200.replicas import Replicas
 
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=device)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    rep = Replicas("nccl", device)
+    barrier = rep.barrier
+    max_over_ranks = rep.max
 
     # inputs resident in HBM, plus pinned host copies for the end-to-end leg
     pinned = [tuple(torch.from_numpy(np.ascontiguousarray(p)).pin_memory() for p in f) for f in host_frames]
@@ -431,7 +420,7 @@ def main():
     step_ms = max_over_ranks(enc_ms + dec_ms)
     enc_ms = max_over_ranks(enc_ms)
     dec_ms = max_over_ranks(dec_ms)
-    value = world * luma / (step_ms / 1e3) / 1e9
+    value = rep.rate(luma, step_ms) / 1e9
 
     peaks = {}
     try:
@@ -473,7 +462,7 @@ def main():
                              list(sp["tile"]) for sp in specs},
                    "tuning": args.tuning, "launch_ctas_per_sm": autotune.launch_settings(),
                    "l2": "inputs 1.3 GB > 126 MB L2 (no flush needed)", "parallelism": f"replicas x{world}"},
-        "enc_gpix_s": world * luma / (enc_ms / 1e3) / 1e9, "dec_gpix_s": world * luma / (dec_ms / 1e3) / 1e9,
+        "enc_gpix_s": rep.rate(luma, enc_ms) / 1e9, "dec_gpix_s": rep.rate(luma, dec_ms) / 1e9,
         "enc_ms": enc_ms, "dec_ms": dec_ms, "stream_bytes": stream_bytes, "bit_exact": bool(bit_exact),
         "roofline": roofline,
         "pipeline_roofline": {"achieved": pipeline, "peak": hbm_peak, "unit": "GB/s", "frac": pipeline / hbm_peak,
@@ -501,7 +490,7 @@ def main():
         b.record()
         b.synchronize()
         plain_ms = max_over_ranks(a.elapsed_time(b))
-        line["plain_gpix_s"] = world * luma / (plain_ms / 1e3) / 1e9
+        line["plain_gpix_s"] = rep.rate(luma, plain_ms) / 1e9
         line["batched_over_plain"] = line["value"] / line["plain_gpix_s"]
 
     # end to end through the public API with host buffers
@@ -532,7 +521,7 @@ def main():
         b.synchronize()
         e2e_ms = max_over_ranks(a.elapsed_time(b) / k_e2e)
         frame_bytes = 2 * samples
-        line["e2e"] = {"value": world * luma / (e2e_ms / 1e3) / 1e9, "unit": "Gpix/s",
+        line["e2e"] = {"value": rep.rate(luma, e2e_ms) / 1e9, "unit": "Gpix/s",
                        "h2d_bytes_per_step": frame_bytes + stream_bytes,
                        "d2h_bytes_per_step": stream_bytes + frame_bytes, "ms_per_step": e2e_ms,
                        "path": "BatchCodec.encode_host (pinned frames -> pinned streams) then decode_host "
@@ -553,8 +542,7 @@ def main():
         line["bit_exact"] = bool(line["bit_exact"] and line["serving"]["bit_exact"])
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    rep.close()
     return 0
 
 
