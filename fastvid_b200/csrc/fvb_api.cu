@@ -919,11 +919,12 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
       dec_other_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), 4, ctas(K_DEC_OTHER)), 128, 0, other>>>(
           frames_d, state, shards, t.shards, lists, items, folded);
     }
-    FVB_LAUNCHED("dec_other_kernel");
-    if (side) {
+    const cudaError_t launched = cudaGetLastError();
+    if (side) {  // joined even when the launch failed, so a stream capture is never left forked
       FVB_CUDA(cudaEventRecord(side->join, other));
       FVB_CUDA(cudaStreamWaitEvent(stream, side->join, 0));
     }
+    if (launched != cudaSuccess) return cuda_fail(launched, "dec_other_kernel");
   }
   if (wavefront) {
     {
