@@ -6,7 +6,11 @@ One step = encode every frame of the batch and decode every stream again,
 inputs resident in HBM (1.3 GB, above the 126 MB L2, so no flush is needed).
 Prints one JSON line (rank 0).  ``--impl reference`` times the CPU restatement
 of the reference codec (the reference has no CPU codec of its own) on all host
-cores over a bounded sample of the same workload.
+cores over the same 96 frames.  The line's ``reference_gpu`` object times the
+reference's own CUDA codec, built from its sources for sm_100 (oracle/_ref),
+through its binding one frame at a time as its public API drives it, beside
+this library's single-frame and batched forms on the same frames;
+``--impl reference_gpu`` prints that leg alone.
 
 Launch: python bench.py [--gpus N] [--steps K] [--warmup W]
         python -m torch.distributed.run --nproc-per-node N ... bench.py --gpus N
@@ -40,16 +44,17 @@ def parse_args():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
-    p.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    p.add_argument("--impl", default="ours", choices=("ours", "reference", "reference_gpu"))
     p.add_argument("--frames", type=int, default=96)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
     p.add_argument("--no-tuning", action="store_true", help="ignore the autotuned table (tiles, launch geometry)")
-    p.add_argument("--serve-requests", type=int, default=2000,
+    p.add_argument("--no-reference-gpu", action="store_true", help="skip the reference GPU leg")
+    p.add_argument("--serve-requests", type=int, default=10000,
                    help="requests of the serving leg (the serving mix; 0 skips it)")
-    p.add_argument("--serve-rates", default="1000,4000,8000,16000,0",
+    p.add_argument("--serve-rates", default="1000,2000,5000,10000,20000,0",
                    help="offered request rates of the serving leg, per second (0: all at once)")
     p.add_argument("--serve-budget-gb", type=float, default=40.0, help="device-memory budget of the server")
     return p.parse_args()
@@ -185,8 +190,8 @@ def serving_leg(args, device):
     return out
 
 
-def cpu_sample(specs):
-    """One frame of each format: the bounded CPU sample."""
+def format_sample(specs):
+    """One frame of each format."""
     seen, out = set(), []
     for i, s in enumerate(specs):
         key = (s["layout"], s["bit_depth"])
@@ -194,6 +199,109 @@ def cpu_sample(specs):
             seen.add(key)
             out.append(i)
     return out
+
+
+LAYOUT_CODES = {"gray": 0, "yuv422": 1, "rgb444": 2}
+
+
+def load_reference_gpu():
+    """The reference's CUDA codec built from its own sources (oracle/_ref),
+    or the reason it is unavailable."""
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    if not os.path.isdir(ref_dir) or not any(f.startswith("fastvid_ref_C") and f.endswith(".so")
+                                             for f in os.listdir(ref_dir)):
+        return None, "reference extension not built (oracle/build_ref.py needs the reference sources)"
+    sys.path.insert(0, ref_dir)
+    try:
+        import fastvid_ref_C
+    except Exception as exc:  # noqa: BLE001 - report why the leg could not run
+        return None, f"reference extension failed to load: {exc}"
+    return fastvid_ref_C, None
+
+
+def event_median(fn, warmup, reps):
+    """The reference evaluator's protocol (scripts/evaluate.py:447-476):
+    warm-ups, then `reps` calls each between two CUDA events with a
+    synchronisation, median milliseconds."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    return statistics.median(times)
+
+
+def plain_and_reference_legs(specs, dev_frames, layouts, depths, quals, tiles, luma, warmup, reps, with_ref,
+                             ours=True):
+    """Per-frame loops over the whole mix (the reference's list API is such a
+    loop, fastvid/__init__.py:44-53): this library's single-frame path and
+    the reference's CUDA build, encode and decode timed separately, plus one
+    frame of each format alone.  Returns (ours, reference) dicts."""
+    import torch
+
+    import fastvid_b200
+
+    def our_enc():
+        return [fastvid_b200.encode(f, layout=layouts[i], bit_depth=depths[i], quality=quals[i], tile_size=tiles[i])
+                for i, f in enumerate(dev_frames)]
+
+    out = {}
+    ref_out = None
+    fmt_idx = format_sample(specs)
+    fmt_name = {i: autotune_key(specs[i]) for i in fmt_idx}
+    if ours:
+        streams = our_enc()
+        enc = event_median(our_enc, warmup, reps)
+        dec = event_median(lambda: [fastvid_b200.decode(s) for s in streams], warmup, reps)
+        out = {"enc_ms": enc, "dec_ms": dec, "gpix_s": luma / (enc + dec) / 1e6,
+               "enc_gpix_s": luma / enc / 1e6, "dec_gpix_s": luma / dec / 1e6, "per_format_ms": {}}
+        for i in fmt_idx:
+            f = dev_frames[i]
+            e = event_median(lambda: fastvid_b200.encode(f, layout=layouts[i], bit_depth=depths[i],
+                                                         quality=quals[i], tile_size=tiles[i]), warmup, reps)
+            d = event_median(lambda: fastvid_b200.decode(streams[i]), warmup, reps)
+            out["per_format_ms"][fmt_name[i]] = {"encode": e, "decode": d}
+    if with_ref:
+        ref, why = load_reference_gpu()
+        if ref is None:
+            return out, {"unavailable": why}
+        frames_l = [list(f) for f in dev_frames]
+
+        def ref_enc_one(i):
+            return ref.encode(frames_l[i], LAYOUT_CODES[layouts[i]], depths[i], quals[i], 24, 1, tiles[i][0],
+                              tiles[i][1])
+
+        def ref_enc():
+            return [ref_enc_one(i) for i in range(len(dev_frames))]
+
+        rstreams = ref_enc()
+        enc = event_median(ref_enc, warmup, reps)
+        dec = event_median(lambda: [ref.decode(s, True) for s in rstreams], warmup, reps)
+        ref_out = {"impl": "reference CUDA codec (cuda/csrc) built for sm_100 from its own sources, called "
+                           "per frame through its binding _C.encode/_C.decode",
+                   "enc_ms": enc, "dec_ms": dec, "gpix_s": luma / (enc + dec) / 1e6,
+                   "enc_gpix_s": luma / enc / 1e6, "dec_gpix_s": luma / dec / 1e6, "per_format_ms": {},
+                   "protocol": f"{warmup} warm-ups, median of {reps} CUDA-event timed calls"}
+        for i in fmt_idx:
+            e = event_median(lambda: ref_enc_one(i), warmup, reps)
+            d = event_median(lambda: ref.decode(rstreams[i], True), warmup, reps)
+            ref_out["per_format_ms"][fmt_name[i]] = {"encode": e, "decode": d}
+        if ours:
+            same = all(torch.equal(a, b) for a, b in zip(streams, rstreams))
+            ref_out["streams_identical_to_ours"] = bool(same)
+    return out, ref_out
+
+
+def autotune_key(spec):
+    return f"{spec['layout']}-{spec['bit_depth']}-{spec['width']}x{spec['height']}"
 
 
 class Clocks:
@@ -279,9 +387,8 @@ def run_reference(args, specs):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    idx = cpu_sample(specs)
-    frames = {i: _gen(specs[i]) for i in idx}
-    fl = [frames.get(i) for i in range(len(specs))]
+    idx = list(range(len(specs)))
+    fl = generate(specs, max(1, min(16, os.cpu_count() or 2)))
     for _ in range(max(1, args.warmup)):
         time_oracle(fl, specs, idx, 0.0)
     t0 = time.perf_counter()
@@ -291,7 +398,7 @@ def run_reference(args, specs):
         values.append(g)
     elapsed = time.perf_counter() - t0
     value = statistics.median(values)
-    sample = f"frames {idx} (one per format) encode+decode per step, {threads} threads"
+    sample = f"all {len(idx)} frames of the mix, encode+decode per step, {threads} threads"
     line = {
         "impl": "reference", "metric": "Gpix/s encode+decode", "value": value, "unit": "Gpix/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -304,6 +411,25 @@ def run_reference(args, specs):
         "e2e": {"value": value, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_gpu(args, specs):
+    """The reference's CUDA build alone over the mix (one GPU, rank 0)."""
+    import numpy as np
+    import torch
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    host = generate(specs, max(1, min(16, os.cpu_count() or 2)))
+    dev = [tuple(torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in f) for f in host]
+    luma = sum(s["width"] * s["height"] for s in specs)
+    _, ref = plain_and_reference_legs(specs, dev, [s["layout"] for s in specs], [s["bit_depth"] for s in specs],
+                                      [s["quality"] for s in specs], [s["tile"] for s in specs], luma,
+                                      max(1, args.warmup), max(1, args.steps), True, ours=False)
+    print(json.dumps({"impl": "reference_gpu", "metric": "Gpix/s encode+decode", "unit": "Gpix/s",
+                      "value": ref.get("gpix_s"), "config": {"workload": WORKLOAD, "frames": len(specs)},
+                      "reference_gpu": ref}), flush=True)
     return 0
 
 
@@ -327,6 +453,8 @@ def main():
     args.tuning = ("autotuned table fastvid_b200/tuning/b200.json" if table else "built-in defaults")
     if args.impl == "reference":
         return run_reference(args, specs)
+    if args.impl == "reference_gpu":
+        return run_reference_gpu(args, specs)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -384,7 +512,7 @@ def main():
     for i, (s, f) in enumerate(zip(specs, dev_frames)):
         if s["quality"] == 100 or (s["bit_depth"] == 8 and s["layout"] == "gray"):
             bit_exact &= all(torch.equal(a, b) for a, b in zip(planes[i], f))
-    for i in cpu_sample(specs):
+    for i in format_sample(specs):
         plain = fastvid_b200.encode(dev_frames[i], layout=layouts[i], bit_depth=depths[i], quality=quals[i],
                                     tile_size=tiles[i])
         bit_exact &= torch.equal(plain, streams[i])
@@ -472,26 +600,23 @@ def main():
         "clocks": clocks.summary(),
     }
 
-    # single-frame (plain, drop-in) path on the same frames, for the batched/plain ratio
+    # single-frame (plain, drop-in) path and the reference's own CUDA build on
+    # the same frames, one call per frame, the reference evaluator's protocol
     if not args.no_plain:
-        def plain_step():
-            out = []
-            for i, f in enumerate(dev_frames):
-                st = fastvid_b200.encode(f, layout=layouts[i], bit_depth=depths[i], quality=quals[i],
-                                         tile_size=tiles[i])
-                out.append(fastvid_b200.decode(st))
-            return out
-
-        plain_step()
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        plain_step()
-        b.record()
-        b.synchronize()
-        plain_ms = max_over_ranks(a.elapsed_time(b))
+        plain, ref_gpu = plain_and_reference_legs(specs, dev_frames, layouts, depths, quals, tiles, luma, 5, 20,
+                                                  rank == 0 and world == 1 and not args.no_reference_gpu)
+        plain_ms = max_over_ranks(plain["enc_ms"] + plain["dec_ms"])
         line["plain_gpix_s"] = rep.rate(luma, plain_ms) / 1e9
+        line["plain"] = plain
         line["batched_over_plain"] = line["value"] / line["plain_gpix_s"]
+        if ref_gpu is not None:
+            if "gpix_s" in ref_gpu:
+                ref_gpu["batched_over_reference_gpu"] = line["value"] / ref_gpu["gpix_s"]
+                ref_gpu["plain_over_reference_gpu"] = plain["gpix_s"] / ref_gpu["gpix_s"]
+                ref_gpu["per_format_plain_over_reference_gpu"] = {
+                    k: {op: ref_gpu["per_format_ms"][k][op] / plain["per_format_ms"][k][op]
+                        for op in ("encode", "decode")} for k in ref_gpu["per_format_ms"]}
+            line["reference_gpu"] = ref_gpu
 
     # end to end through the public API with host buffers
     if not args.no_e2e:
@@ -532,10 +657,10 @@ def main():
 
     # CPU baseline: the oracle (restatement of the reference) on all host cores
     if rank == 0 and world == 1 and not args.no_cpu:
-        idx = cpu_sample(specs)
+        idx = list(range(len(specs)))
         gpix, threads, reps = time_oracle(host_frames, specs, idx, args.cpu_seconds)
         line["cpu_baseline"] = {"value": gpix, "unit": "Gpix/s", "cores": threads, "kind": "port",
-                                "sample": f"frames {idx} (one per format), encode+decode, {reps} reps"}
+                                "sample": f"all {len(idx)} frames of the mix, encode+decode, {reps} reps"}
     # serving form (one GPU): continuous batching at offered rates, p50/p99
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serving"] = serving_leg(args, device)

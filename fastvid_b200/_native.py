@@ -36,6 +36,20 @@ class Frame(ctypes.Structure):
         return other
 
 
+class Bucket(ctypes.Structure):
+    """Mirror of ``fvb_bucket``: a capacity that a batch fits (see the header)."""
+
+    _fields_ = [
+        ("frames", c_i64), ("tiles", c_i64), ("shards", c_i64), ("samples", c_i64), ("prefix", c_i64),
+        ("frames_p", c_i64 * 3), ("tiles_p", c_i64 * 3), ("shards_p", c_i64 * 3),
+        ("passes", c_i32), ("wide", c_i32),
+    ]
+
+    def key(self) -> tuple:
+        return (self.frames, self.tiles, self.shards, self.samples, self.prefix, tuple(self.frames_p),
+                tuple(self.tiles_p), tuple(self.shards_p), self.passes, self.wide)
+
+
 # exported symbol -> (argtypes, restype)
 SIGNATURES = {
     "fvb_abi_version": ([], c_i32),
@@ -63,6 +77,16 @@ SIGNATURES = {
     "fvb_batch_decode_plan": ([ctypes.POINTER(Frame), c_i32, ctypes.POINTER(c_i64)], c_i32),
     "fvb_batch_decode_prepare": ([ctypes.POINTER(Frame), c_i32, c_p, c_p, c_p, c_p, c_p, c_i64, c_p], c_i32),
     "fvb_batch_decode_enqueue": ([ctypes.POINTER(Frame), c_i32, c_i32, c_p, c_i64, c_p, c_p], c_i32),
+    "fvb_batch_bucket": ([ctypes.POINTER(Frame), c_i32, ctypes.POINTER(Bucket)], c_i32),
+    "fvb_bucket_encode_plan": ([ctypes.POINTER(Bucket), ctypes.POINTER(c_i64)], c_i32),
+    "fvb_bucket_decode_plan": ([ctypes.POINTER(Bucket), ctypes.POINTER(c_i64)], c_i32),
+    "fvb_bucket_encode_prepare": ([ctypes.POINTER(Bucket), ctypes.POINTER(Frame), c_i32, c_p, c_p, c_p, c_i64, c_p],
+                                  c_i32),
+    "fvb_bucket_encode_enqueue": ([ctypes.POINTER(Bucket), c_p, c_i64, c_p, c_p], c_i32),
+    "fvb_bucket_encode_emit": ([ctypes.POINTER(Bucket), ctypes.POINTER(Frame), c_i32, c_p, c_i64, c_p, c_p], c_i32),
+    "fvb_bucket_decode_prepare": ([ctypes.POINTER(Bucket), ctypes.POINTER(Frame), c_i32, c_p, c_p, c_p, c_p, c_p,
+                                   c_i64, c_p], c_i32),
+    "fvb_bucket_decode_enqueue": ([ctypes.POINTER(Bucket), c_i32, c_p, c_i64, c_p, c_p], c_i32),
 }
 
 _lib = None

@@ -17,7 +17,7 @@ import torch
 
 from . import decode as _decode
 from . import encode as _encode
-from .batch import decode_batch, encode_batch
+from .batch import decode_batch, encode_batch, stream_headers
 
 _LAYOUT_TO_FORMAT = {0: "gray", 1: "yuv422", 2: "rgb444"}
 
@@ -48,8 +48,8 @@ def decode(encoded):
     streams = list(encoded)
     if not streams:
         return []
-    if any(not s.is_cuda for s in streams):
-        return [_decode(s) for s in streams]
+    # host-resident streams join the batch: uploaded without blocking, their
+    # headers read on the host
     return [tuple(planes) for planes in decode_batch(streams)]
 
 
@@ -57,7 +57,22 @@ def inspect(encoded) -> dict[str, int | str]:
     """Self-described frame metadata and exact overhead accounting (fastvid/__init__.py:66-87)."""
     if not isinstance(encoded, torch.Tensor) or encoded.dtype != torch.uint8 or encoded.ndim != 1:
         raise TypeError("encoded must be a one-dimensional uint8 tensor")
-    header = bytes(encoded[:32].cpu().numpy())
+    return _describe(bytes(encoded[:32].cpu().numpy()))
+
+
+def inspect_batch(streams) -> list[dict[str, int | str]]:
+    """inspect() of every stream of a sequence (no reference counterpart: the
+    reference inspects one stream per call).  The headers of the device
+    streams come back with one gather kernel and one copy for all of them;
+    the same checks and errors as inspect()."""
+    streams = list(streams)
+    for s in streams:
+        if not isinstance(s, torch.Tensor) or s.dtype != torch.uint8 or s.ndim != 1:
+            raise TypeError("encoded must be a one-dimensional uint8 tensor")
+    return [_describe(h) for h in stream_headers(streams)]
+
+
+def _describe(header: bytes) -> dict[str, int | str]:
     if len(header) != 32 or header[:4] != b"FVID" or header[4] != 1:
         raise ValueError("not a Fastvid supported stream")
     layout = header[5]
@@ -76,4 +91,4 @@ def inspect(encoded) -> dict[str, int | str]:
     }
 
 
-__all__ = ["decode", "encode", "inspect"]
+__all__ = ["decode", "encode", "inspect", "inspect_batch"]

@@ -6,10 +6,14 @@ Here a batch of frames of any mix of sizes, layouts and depths goes through
 one persistent launch per kernel: the predictor and reconstruction kernels
 drain a device work queue of tiles from all frames, the analysis, rANS and
 emission kernels cover every shard of every frame, and the frame policy runs
-on the device.  The analysis passes of a batch shape are captured once as a
-CUDA graph and replayed; the host waits once per batch (the stream lengths),
-then launches emission into one exact-size arena.  Streams are byte-identical
-to the single-frame path frame by frame.
+on the device.  Launches are sized by a shape bucket -- the batch's frame,
+tile, shard and sample counts rounded up to steps of at most 25 percent
+(fvb_batch_bucket) -- and the kernels read the batch's actual counts from the
+workspace, so the analysis passes and the decode of a bucket are captured
+once as CUDA graphs and replayed for every batch that falls into it, whatever
+its mix of frames.  The host waits once per batch (the stream lengths), then
+launches emission into one exact-size arena.  Streams are byte-identical to
+the single-frame path frame by frame.
 """
 
 from __future__ import annotations
@@ -20,7 +24,7 @@ from dataclasses import dataclass, field
 import torch
 
 from . import _native
-from ._native import Frame
+from ._native import Bucket, Frame
 from .codec import _LAYOUTS_DEFAULT, plan_encode, plan_decode, plane_views
 
 
@@ -32,38 +36,25 @@ def _per_frame(value, n, name):
 
 
 @dataclass
-class _EncodeSlot:
-    """Cached resources of one batch shape (geometry of every frame)."""
-    frames: ctypes.Array
-    n: int
+class _Slot:
+    """Cached resources of one shape bucket (encode or decode)."""
+    bucket: Bucket
     ws_bytes: int
     workspace: torch.Tensor
-    results: torch.Tensor            # pinned int64 [n, 2]
+    results: torch.Tensor            # pinned int64 [bucket.frames, 2]
+    wavefront: bool = True
     graph: torch.cuda.CUDAGraph | None = None
     stream: torch.cuda.Stream | None = None
     kernels: int = 0                 # kernel launches captured in the graph
-    last_ptrs: tuple = field(default_factory=tuple)
-
-
-@dataclass
-class _DecodeSlot:
-    frames: ctypes.Array
-    n: int
-    ws_bytes: int
-    workspace: torch.Tensor
-    results: torch.Tensor
-    wavefront: bool
-    graph: torch.cuda.CUDAGraph | None = None
-    stream: torch.cuda.Stream | None = None
-    kernels: int = 0
 
 
 class BatchCodec:
     """Batched encoder/decoder bound to one CUDA device.
 
     Resources (workspace, pinned result buffer, CUDA graph) are cached per
-    batch shape, so steady-state calls of a repeated shape allocate nothing
-    but their outputs and issue one graph launch for all analysis passes.
+    shape bucket, so steady-state calls of batches falling into a seen bucket
+    allocate nothing but their outputs and issue one graph launch for all
+    analysis passes (and one for the whole decode).
     """
 
     def __init__(self, device=None, use_graphs: bool = True, max_cached_shapes: int = 8,
@@ -120,31 +111,59 @@ class BatchCodec:
             self._ws_buf = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8, device=self.device)
         return self._ws_buf[:nbytes]
 
+    # ---- buckets ----------------------------------------------------------
+    def _frame_array(self, frames_py: list[Frame]):
+        return (Frame * len(frames_py))(*frames_py)
+
+    def _slot(self, cache: dict, arr, n: int, decode: bool, wavefront: bool = True) -> _Slot:
+        bucket = Bucket()
+        _native.check(self.lib.fvb_batch_bucket(arr, n, ctypes.byref(bucket)))
+        key = (decode, wavefront) + bucket.key()
+        slot = cache.get(key)
+        if slot is not None:
+            return slot
+        ws = ctypes.c_int64()
+        plan = self.lib.fvb_bucket_decode_plan if decode else self.lib.fvb_bucket_encode_plan
+        _native.check(plan(ctypes.byref(bucket), ctypes.byref(ws)))
+        workspace = self._workspace(ws.value)
+        slot = _Slot(bucket, ws.value, workspace, self._results(bucket.frames), wavefront)
+        if len(cache) >= self.max_cached:
+            cache.pop(next(iter(cache)))
+        cache[key] = slot
+        return slot
+
+    def _run_slot(self, slot: _Slot, enqueue, cur) -> None:
+        """Run `enqueue(stream_handle)` for this slot: captured as a graph on
+        the slot's first use (after one eager run), replayed afterwards."""
+        if not self.use_graphs:
+            enqueue(cur.cuda_stream)
+            return
+        if slot.graph is None:
+            slot.stream = torch.cuda.Stream(self.device)
+            slot.stream.wait_stream(cur)
+            # one eager run first (it sets kernel attributes), then capture
+            with torch.cuda.stream(slot.stream):
+                enqueue(slot.stream.cuda_stream)
+            slot.stream.synchronize()
+            graph = torch.cuda.CUDAGraph()
+            k0 = _native.launch_count()
+            # thread-local capture: other threads (serving workers) may keep
+            # launching and allocating on their own streams meanwhile
+            with torch.cuda.graph(graph, stream=slot.stream, capture_error_mode="thread_local"):
+                enqueue(slot.stream.cuda_stream)
+            slot.kernels = _native.launch_count() - k0
+            slot.graph = graph
+        else:
+            slot.stream.wait_stream(cur)
+            with torch.cuda.stream(slot.stream):
+                slot.graph.replay()
+            self.graph_kernels += slot.kernels
+        cur.wait_stream(slot.stream)
+
     # ---- encode -----------------------------------------------------------
     @staticmethod
     def _enc_shape(f: Frame) -> tuple:
         return (f.layout, f.bit_depth, f.quality, f.width, f.height, f.tile_w, f.tile_h, f.fps_num, f.fps_den)
-
-    def _encode_slot(self, frames_py: list[Frame], shapes: list | None = None) -> _EncodeSlot:
-        key = tuple(shapes) if shapes is not None else tuple(self._enc_shape(f) for f in frames_py)
-        slot = self._enc.get(key)
-        if slot is not None:
-            return slot
-        n = len(frames_py)
-        arr = (Frame * n)(*frames_py)
-        ws = ctypes.c_int64()
-        _native.check(self.lib.fvb_batch_encode_plan(arr, n, ctypes.byref(ws)))
-        workspace = self._workspace(ws.value)
-        results = self._results(n)
-        slot = _EncodeSlot(arr, n, ws.value, workspace, results)
-        if len(self._enc) >= self.max_cached:
-            self._enc.pop(next(iter(self._enc)))
-        self._enc[key] = slot
-        return slot
-
-    def _enqueue_encode(self, slot: _EncodeSlot, stream_handle: int):
-        _native.check(self.lib.fvb_batch_encode_enqueue(slot.frames, slot.n, slot.workspace.data_ptr(),
-                                                        slot.ws_bytes, slot.results.data_ptr(), stream_handle))
 
     def encode(self, frames, *, layout=None, bit_depth=10, quality=90, frame_rate=(24, 1), tile_size=(256, 128)):
         """Encode a list of frames (each a tuple of CUDA uint16 planes).
@@ -192,37 +211,18 @@ class BatchCodec:
             pitches.extend(pit)
             pitches.extend((0,) * (3 - len(pit)))
         with torch.cuda.device(self.device):
-            slot = self._encode_slot(plans, shapes)
+            arr = self._frame_array(plans)
+            slot = self._slot(self._enc, arr, n, decode=False)
+            bucket = ctypes.byref(slot.bucket)
             cur = torch.cuda.current_stream(self.device)
             p_arr = (ctypes.c_void_p * (3 * n))(*ptrs)
             q_arr = (ctypes.c_int64 * (3 * n))(*pitches)
-            _native.check(self.lib.fvb_batch_encode_prepare(slot.frames, n, p_arr, q_arr, slot.workspace.data_ptr(),
-                                                            slot.ws_bytes, cur.cuda_stream))
-            if self.use_graphs:
-                if slot.graph is None:
-                    slot.stream = torch.cuda.Stream(self.device)
-                    slot.stream.wait_stream(cur)
-                    # one eager run first (it sets kernel attributes), then capture
-                    with torch.cuda.stream(slot.stream):
-                        self._enqueue_encode(slot, slot.stream.cuda_stream)
-                    slot.stream.synchronize()
-                    graph = torch.cuda.CUDAGraph()
-                    k0 = _native.launch_count()
-                    with torch.cuda.graph(graph, stream=slot.stream):
-                        self._enqueue_encode(slot, slot.stream.cuda_stream)
-                    slot.kernels = _native.launch_count() - k0
-                    slot.graph = graph
-                    cur.wait_stream(slot.stream)
-                slot.stream.wait_stream(cur)
-                with torch.cuda.stream(slot.stream):
-                    slot.graph.replay()
-                self.graph_kernels += slot.kernels
-                slot.stream.synchronize()
-                cur.wait_stream(slot.stream)
-            else:
-                self._enqueue_encode(slot, cur.cuda_stream)
-                cur.synchronize()
-            res = slot.results.tolist()
+            _native.check(self.lib.fvb_bucket_encode_prepare(bucket, arr, n, p_arr, q_arr, slot.workspace.data_ptr(),
+                                                             slot.ws_bytes, cur.cuda_stream))
+            self._run_slot(slot, lambda h: _native.check(self.lib.fvb_bucket_encode_enqueue(
+                bucket, slot.workspace.data_ptr(), slot.ws_bytes, slot.results.data_ptr(), h)), cur)
+            cur.synchronize()
+            res = slot.results[:n].tolist()
             for i, (status, _) in enumerate(res):
                 if status:
                     raise RuntimeError(f"frame {i}: CUDA encoder analysis failed (status {status})")
@@ -234,8 +234,8 @@ class BatchCodec:
                 outs.append(base + off)
                 off += length
             o_arr = (ctypes.c_void_p * n)(*outs)
-            _native.check(self.lib.fvb_batch_encode_emit(slot.frames, n, slot.workspace.data_ptr(), slot.ws_bytes,
-                                                         o_arr, cur.cuda_stream))
+            _native.check(self.lib.fvb_bucket_encode_emit(bucket, arr, n, slot.workspace.data_ptr(), slot.ws_bytes,
+                                                          o_arr, cur.cuda_stream))
             views, off = [], 0  # made while the GPU emits
             for length in lengths:
                 views.append(arena.narrow(0, off, length))
@@ -247,28 +247,6 @@ class BatchCodec:
     def _dec_shape(f: Frame) -> tuple:
         return (f.layout, f.bit_depth, f.quality, f.flags, f.width, f.height, f.tile_w, f.tile_h)
 
-    def _decode_slot(self, frames_py: list[Frame], wavefront: bool, shapes: list | None = None) -> _DecodeSlot:
-        key = (wavefront,) + (tuple(shapes) if shapes is not None else tuple(self._dec_shape(f) for f in frames_py))
-        slot = self._dec.get(key)
-        if slot is not None:
-            return slot
-        n = len(frames_py)
-        arr = (Frame * n)(*frames_py)
-        ws = ctypes.c_int64()
-        _native.check(self.lib.fvb_batch_decode_plan(arr, n, ctypes.byref(ws)))
-        workspace = self._workspace(ws.value)
-        results = self._results(n)
-        slot = _DecodeSlot(arr, n, ws.value, workspace, results, wavefront)
-        if len(self._dec) >= self.max_cached:
-            self._dec.pop(next(iter(self._dec)))
-        self._dec[key] = slot
-        return slot
-
-    def _enqueue_decode(self, slot: _DecodeSlot, stream_handle: int):
-        _native.check(self.lib.fvb_batch_decode_enqueue(slot.frames, slot.n, 1 if slot.wavefront else 0,
-                                                        slot.workspace.data_ptr(), slot.ws_bytes,
-                                                        slot.results.data_ptr(), stream_handle))
-
     def decode(self, streams, predictor="wavefront", headers=None):
         """Decode a list of 1-D uint8 streams; returns a list of plane tuples.
         `headers`: the streams' first 32 bytes when the caller has them
@@ -278,14 +256,27 @@ class BatchCodec:
         n = len(streams)
         if n == 0:
             return []
-        dev_streams = []
+        dev_streams, host_heads = [], []
         for s in streams:
             if s.dtype != torch.uint8 or s.dim() != 1:
                 raise RuntimeError("encoded must be a one-dimensional uint8 tensor")
             if s.numel() < 32:
                 raise RuntimeError("truncated Fastvid header")
             s = s.contiguous()
-            dev_streams.append(s if s.device == self.device else s.to(self.device))
+            if s.device == self.device:
+                dev_streams.append(s)
+                host_heads.append(None)
+            elif not s.is_cuda:
+                # a host stream: its header is read here, its bytes uploaded
+                # without blocking (ordered before the decode on this stream)
+                host_heads.append(bytes(s[:32].numpy().tobytes()))
+                with torch.cuda.device(self.device):
+                    dev_streams.append(s.to(self.device, non_blocking=s.is_pinned()))
+            else:
+                dev_streams.append(s.to(self.device))
+                host_heads.append(None)
+        if headers is None and all(h is not None for h in host_heads):
+            headers = host_heads
         with torch.cuda.device(self.device):
             cur = torch.cuda.current_stream(self.device)
             need = ((16 * n + 255) // 256) * 256 + 32 * n
@@ -316,7 +307,10 @@ class BatchCodec:
                 plans.append(hit)
                 shapes.append(hit[1])
                 sizes.append(hit[2])
-            slot = self._decode_slot([h[0] for h in plans], predictor == "wavefront", shapes)
+            arr = self._frame_array([h[0] for h in plans])
+            wavefront = predictor == "wavefront"
+            slot = self._slot(self._dec, arr, n, decode=True, wavefront=wavefront)
+            bucket = ctypes.byref(slot.bucket)
             total = sum(sizes)
             arena = torch.empty(total, dtype=torch.uint16, device=self.device)
             # plane pointers by arithmetic (Y, then Cb, then Cr of each frame);
@@ -332,44 +326,19 @@ class BatchCodec:
                 off += samples
             p_arr = (ctypes.c_void_p * (3 * n))(*ptrs)
             q_arr = (ctypes.c_int64 * (3 * n))(*pitches)
-            _native.check(self.lib.fvb_batch_decode_prepare(slot.frames, n, s_arr, l_arr, p_arr, q_arr,
-                                                            slot.workspace.data_ptr(), slot.ws_bytes,
-                                                            cur.cuda_stream))
-            def views():
-                out, off = [], 0
-                for f, _, samples, *_ in plans:
-                    out.append(tuple(plane_views(arena.narrow(0, off, samples), f)))
-                    off += samples
-                return out
-
-            if self.use_graphs:
-                if slot.graph is None:
-                    slot.stream = torch.cuda.Stream(self.device)
-                    slot.stream.wait_stream(cur)
-                    with torch.cuda.stream(slot.stream):
-                        self._enqueue_decode(slot, slot.stream.cuda_stream)
-                    slot.stream.synchronize()
-                    graph = torch.cuda.CUDAGraph()
-                    k0 = _native.launch_count()
-                    with torch.cuda.graph(graph, stream=slot.stream):
-                        self._enqueue_decode(slot, slot.stream.cuda_stream)
-                    slot.kernels = _native.launch_count() - k0
-                    slot.graph = graph
-                    cur.wait_stream(slot.stream)
-                    # the eager run above already decoded this batch
-                else:
-                    slot.stream.wait_stream(cur)
-                    with torch.cuda.stream(slot.stream):
-                        slot.graph.replay()
-                    self.graph_kernels += slot.kernels
-                out_planes = views()
-                slot.stream.synchronize()
-                cur.wait_stream(slot.stream)
-            else:
-                self._enqueue_decode(slot, cur.cuda_stream)
-                out_planes = views()
-                cur.synchronize()
-            for i, (status, _) in enumerate(slot.results.tolist()):
+            _native.check(self.lib.fvb_bucket_decode_prepare(bucket, arr, n, s_arr, l_arr, p_arr, q_arr,
+                                                             slot.workspace.data_ptr(), slot.ws_bytes,
+                                                             cur.cuda_stream))
+            self._run_slot(slot, lambda h: _native.check(self.lib.fvb_bucket_decode_enqueue(
+                bucket, 1 if wavefront else 0, slot.workspace.data_ptr(), slot.ws_bytes, slot.results.data_ptr(),
+                h)), cur)
+            out_planes = []
+            off = 0
+            for f, _, samples, *_ in plans:
+                out_planes.append(tuple(plane_views(arena.narrow(0, off, samples), f)))
+                off += samples
+            cur.synchronize()
+            for i, (status, _) in enumerate(slot.results[:n].tolist()):
                 if status:
                     raise RuntimeError(f"frame {i}: malformed entropy payload (CUDA status {status})")
         return out_planes
@@ -510,6 +479,34 @@ class BatchCodec:
         return res
 
 
+    def headers(self, streams) -> list[bytes]:
+        """The 32-byte header of each stream (shorter streams: their bytes):
+        CPU streams read in place, this device's streams with one gather
+        kernel and one copy for all of them."""
+        out: list = [None] * len(streams)
+        dev = []
+        for i, s in enumerate(streams):
+            if s.is_cuda and s.device == self.device:
+                dev.append(i)
+            else:
+                out[i] = bytes(s[:32].cpu().numpy().tobytes())
+        if dev:
+            n = len(dev)
+            with torch.cuda.device(self.device):
+                cur = torch.cuda.current_stream(self.device)
+                need = ((16 * n + 255) // 256) * 256 + 32 * n
+                if self._hdr_scratch is None or self._hdr_scratch.numel() < need:
+                    self._hdr_scratch = torch.empty(max(need, 1 << 16), dtype=torch.uint8, device=self.device)
+                s_arr = (ctypes.c_void_p * n)(*[streams[i].contiguous().data_ptr() for i in dev])
+                l_arr = (ctypes.c_int64 * n)(*[streams[i].numel() for i in dev])
+                heads = ctypes.create_string_buffer(32 * n)
+                _native.check(self.lib.fvb_gather_headers(s_arr, l_arr, n, self._hdr_scratch.data_ptr(),
+                                                          self._hdr_scratch.numel(), heads, cur.cuda_stream))
+            for k, i in enumerate(dev):
+                out[i] = heads.raw[32 * k:32 * k + min(32, streams[i].numel())]
+        return out
+
+
 _default: dict = {}
 
 
@@ -534,5 +531,15 @@ def decode_batch(streams, predictor="wavefront"):
     """Decode a list of streams with the per-device default BatchCodec."""
     if not streams:
         return []
-    dev = streams[0].device if streams[0].is_cuda else None
+    dev = next((s.device for s in streams if s.is_cuda), None)
     return default_codec(dev).decode(streams, predictor)
+
+
+def stream_headers(streams) -> list[bytes]:
+    """Headers of a list of streams (see BatchCodec.headers)."""
+    if not streams:
+        return []
+    cuda = [s for s in streams if s.is_cuda]
+    if not cuda:
+        return [bytes(s[:32].numpy().tobytes()) for s in streams]
+    return default_codec(cuda[0].device).headers(streams)

@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes
 import operator
+import threading
 
 import torch
 
@@ -160,15 +161,57 @@ def plane_views(output: torch.Tensor, frame: Frame):
     return planes
 
 
+_STAGE_CHUNK = 1 << 20
+_staging = threading.local()
+
+
+def _upload(host: torch.Tensor, device: torch.device) -> torch.Tensor:
+    """Copy a CPU stream to the device on the current stream without
+    blocking on the transfer.  A pinned tensor is copied directly; a pageable
+    one goes through two pinned 1 MiB staging halves kept per thread: the
+    host fills one half while the other is in flight, so host copying and
+    the transfer overlap.  The caller's decode waits for its status word,
+    which orders these copies before the staging is reused."""
+    out = torch.empty(host.numel(), dtype=torch.uint8, device=device)
+    if host.is_pinned() or host.numel() <= 4096:
+        out.copy_(host, non_blocking=host.is_pinned())
+        return out
+    per_device = getattr(_staging, "by_device", None)
+    if per_device is None:
+        per_device = _staging.by_device = {}
+    stage = per_device.get(device.index)
+    if stage is None:
+        stage = per_device[device.index] = (torch.empty(2 * _STAGE_CHUNK, dtype=torch.uint8).pin_memory(),
+                                            [torch.cuda.Event(), torch.cuda.Event()])
+    buf, events = stage
+    stream = torch.cuda.current_stream(device)
+    # (the previous call's transfers ended before it returned: its decode
+    # waited for its status word on this stream)
+    for k, lo in enumerate(range(0, host.numel(), _STAGE_CHUNK)):
+        n = min(_STAGE_CHUNK, host.numel() - lo)
+        half = buf.narrow(0, (k & 1) * _STAGE_CHUNK, n)
+        events[k & 1].synchronize()  # this half's previous transfer has landed (no-op before its first use)
+        half.copy_(host.narrow(0, lo, n))
+        out.narrow(0, lo, n).copy_(half, non_blocking=True)
+        events[k & 1].record(stream)
+    return out
+
+
 def decode_frame(encoded: torch.Tensor, wavefront: bool = True):
-    """Decode one stream (CPU or CUDA uint8) to a list of CUDA uint16 planes."""
+    """Decode one stream (CPU or CUDA uint8) to a list of CUDA uint16 planes.
+
+    A CPU stream is validated from its host header (fastvid_cuda.cpp:142-183)
+    and uploaded without blocking (see _upload), so the host plans the frame
+    and allocates its outputs while the bytes are in flight; the device
+    metadata parse then runs on the uploaded copy."""
     frame, ws_bytes = plan_decode(encoded)
     if encoded.is_cuda:
         device = encoded.device
         stream_dev = encoded.contiguous()
     else:
         device = torch.device("cuda", torch.cuda.current_device())
-        stream_dev = encoded.contiguous().to(device)
+        with torch.cuda.device(device):
+            stream_dev = _upload(encoded.contiguous(), device)
     lib = _native.load()
     with torch.cuda.device(device):
         output = torch.empty(frame.samples, dtype=torch.uint16, device=device)

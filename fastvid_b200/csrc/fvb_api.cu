@@ -281,6 +281,10 @@ int ensure_smem_attrs() {
                                 static_cast<int>(dec_reconstruct_smem())));
   FVB_CUDA(cudaFuncSetAttribute(dec_rans_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(dec_rans_smem())));
+  // the whole unified L1/shared array as shared memory: four dec_rans CTAs
+  // (56 KB each) per SM
+  FVB_CUDA(cudaFuncSetAttribute(dec_rans_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared));
   if (dev >= 0 && dev < 64) done[dev] = true;
   return FVB_OK;
 }
@@ -299,7 +303,11 @@ int frame_passes(const fvb_frame& f) {
 }
 constexpr int kMaxPasses = 3;
 
+// Work of a batch, or the capacity of a bucket of batches (layouts and
+// launch grids are sized by capacity; kernels read the actual counts from
+// the BatchDims record in the workspace).
 struct Totals {
+  int frames = 0;
   int64_t tiles = 0, shards = 0, samples = 0, prefix = 0;
   bool wide = false;
   int passes = 1;
@@ -311,6 +319,7 @@ struct Totals {
 
 Totals totals_of(const fvb_frame* frames, int n) {
   Totals t;
+  t.frames = n;
   for (int i = 0; i < n; ++i) {
     const fvb_frame& f = frames[i];
     t.tiles += f.tiles;
@@ -341,11 +350,101 @@ std::vector<int> encode_order(const fvb_frame* frames, int n) {
   return order;
 }
 
+BatchDims dims_of(const Totals& t) {
+  BatchDims d{};
+  for (int p = 0; p < kMaxPasses; ++p) {
+    d.frames_p[p] = t.frames_p[p];
+    d.tiles_p[p] = t.tiles_p[p];
+    d.shards_p[p] = t.shards_p[p];
+  }
+  d.frames_p[0] = t.frames;
+  d.tiles_p[0] = t.tiles;
+  d.shards_p[0] = t.shards;
+  d.passes = t.passes;
+  d.samples = t.samples;
+  return d;
+}
+
+// A batch fits a capacity when every count is within it and the launch
+// sequence is the same (encoder passes, wide-tile kernels).
+bool fits(const Totals& a, const Totals& cap) {
+  if (a.frames > cap.frames || a.tiles > cap.tiles || a.shards > cap.shards || a.samples > cap.samples ||
+      a.prefix > cap.prefix || a.passes != cap.passes || a.wide != cap.wide)
+    return false;
+  for (int p = 0; p < kMaxPasses; ++p)
+    if (a.frames_p[p] > cap.frames_p[p] || a.tiles_p[p] > cap.tiles_p[p] || a.shards_p[p] > cap.shards_p[p])
+      return false;
+  return true;
+}
+
+// Bucket capacity: v rounded up to m * 2^e with m in 4..8 (the capacity is
+// at most 25 percent above v), and at least `floor`.
+int64_t bucket_round(int64_t v, int64_t floor) {
+  if (v <= floor) return floor;
+  int e = 0;
+  while ((v >> e) > 7) ++e;                                  // v >> e in 4..7 once v >= 8
+  const int64_t m = (v + (int64_t{1} << e) - 1) >> e;        // ceil(v / 2^e) in 4..8
+  return m << e;
+}
+
+Totals bucket_of(const Totals& t) {
+  Totals b = t;
+  b.frames = static_cast<int>(bucket_round(t.frames, 1));
+  b.tiles = bucket_round(t.tiles, 16);
+  b.shards = bucket_round(t.shards, 16);
+  b.samples = bucket_round(t.samples, 1 << 16);
+  b.prefix = bucket_round(t.prefix, 1 << 12);
+  for (int p = 0; p < kMaxPasses; ++p) {
+    b.frames_p[p] = t.frames_p[p] ? static_cast<int>(bucket_round(t.frames_p[p], 1)) : 0;
+    b.tiles_p[p] = t.tiles_p[p] ? bucket_round(t.tiles_p[p], 16) : 0;
+    b.shards_p[p] = t.shards_p[p] ? bucket_round(t.shards_p[p], 16) : 0;
+  }
+  return b;
+}
+
+void to_bucket(const Totals& t, fvb_bucket* b) {
+  std::memset(b, 0, sizeof(*b));
+  b->frames = t.frames;
+  b->tiles = t.tiles;
+  b->shards = t.shards;
+  b->samples = t.samples;
+  b->prefix = t.prefix;
+  for (int p = 0; p < kMaxPasses; ++p) {
+    b->frames_p[p] = t.frames_p[p];
+    b->tiles_p[p] = t.tiles_p[p];
+    b->shards_p[p] = t.shards_p[p];
+  }
+  b->passes = t.passes;
+  b->wide = t.wide ? 1 : 0;
+}
+
+int from_bucket(const fvb_bucket* b, Totals* t) {
+  if (!b || b->frames <= 0 || b->frames > (1 << 24) || b->tiles < 0 || b->shards < 0 || b->samples < 0 ||
+      b->prefix < 0 || b->passes < 1 || b->passes > kMaxPasses)
+    return fail(FVB_ERR_ARGUMENT, "invalid bucket");
+  *t = Totals{};
+  t->frames = static_cast<int>(b->frames);
+  t->tiles = b->tiles;
+  t->shards = b->shards;
+  t->samples = b->samples;
+  t->prefix = b->prefix;
+  for (int p = 0; p < kMaxPasses; ++p) {
+    if (b->frames_p[p] < 0 || b->frames_p[p] > b->frames || b->tiles_p[p] < 0 || b->shards_p[p] < 0)
+      return fail(FVB_ERR_ARGUMENT, "invalid bucket");
+    t->frames_p[p] = static_cast<int>(b->frames_p[p]);
+    t->tiles_p[p] = b->tiles_p[p];
+    t->shards_p[p] = b->shards_p[p];
+  }
+  t->passes = b->passes;
+  t->wide = b->wide != 0;
+  return FVB_OK;
+}
+
 struct EncLayout {
-  size_t frames, state, outs, queue, results, shards, folded, rans, prefix, recon, total;
+  size_t dims, frames, state, outs, queue, results, shards, folded, rans, prefix, recon, total;
 };
 
-EncLayout enc_layout(int n, const Totals& t) {
+EncLayout enc_layout(const Totals& t) {
   EncLayout w;
   size_t o = 0;
   auto take = [&](size_t bytes) {
@@ -353,6 +452,8 @@ EncLayout enc_layout(int n, const Totals& t) {
     o = align_up(o + bytes);
     return r;
   };
+  const size_t n = static_cast<size_t>(t.frames);
+  w.dims = take(sizeof(BatchDims));
   w.frames = take(sizeof(FrameDesc) * n);
   w.state = take(sizeof(FrameState) * n);
   w.outs = take(sizeof(uint8_t*) * n);
@@ -368,10 +469,10 @@ EncLayout enc_layout(int n, const Totals& t) {
 }
 
 struct DecLayout {
-  size_t frames, state, queue, results, shards, lists, items, tables, folded, total;
+  size_t dims, frames, state, queue, results, shards, lists, items, tables, folded, total;
 };
 
-DecLayout dec_layout(int n, const Totals& t) {
+DecLayout dec_layout(const Totals& t) {
   DecLayout w;
   size_t o = 0;
   auto take = [&](size_t bytes) {
@@ -379,6 +480,8 @@ DecLayout dec_layout(int n, const Totals& t) {
     o = align_up(o + bytes);
     return r;
   };
+  const size_t n = static_cast<size_t>(t.frames);
+  w.dims = take(sizeof(BatchDims));
   w.frames = take(sizeof(FrameDesc) * n);
   w.state = take(sizeof(FrameState) * n);
   w.queue = take(kAlign);
@@ -400,8 +503,9 @@ __global__ void gather_headers_kernel(const uint8_t* const* __restrict__ streams
   out[i] = b < lens[k] ? streams[k][b] : 0;
 }
 
-__global__ void results_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state, int n,
-                               int64_t* __restrict__ out, int decode) {
+__global__ void results_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
+                               const BatchDims* __restrict__ dims, int64_t* __restrict__ out, int decode) {
+  const int n = dims->frames_p[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int slot = frames[i].slot;
@@ -409,11 +513,46 @@ __global__ void results_kernel(const FrameDesc* __restrict__ frames, const Frame
   out[2 * slot + 1] = decode ? 0 : state[i].stream_len;
 }
 
+// Restores the caller's current device when an entry point returns: the
+// library launches on the device that owns the workspace and switches to it
+// for the call only.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      prev = -1;
+      cudaGetLastError();
+    }
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
+// The device that a kernel can read `p` on: device memory, or managed memory
+// (its preferred device); -1 for host, pinned-host or unknown pointers, which
+// a kernel of this library must never be given.
+int device_of(const void* p) {
+  if (!p) return -1;
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  if (attr.type == cudaMemoryTypeDevice) return attr.device;
+  if (attr.type == cudaMemoryTypeManaged) return attr.device >= 0 ? attr.device : 0;
+  return -1;
+}
+
 int check_ws(void* ws, int64_t ws_bytes, size_t need) {
   if (!ws || ws_bytes < static_cast<int64_t>(need))
     return fail(FVB_ERR_WORKSPACE, "workspace is smaller than planned");
   if (reinterpret_cast<uintptr_t>(ws) & (kAlign - 1)) return fail(FVB_ERR_WORKSPACE, "workspace must be 256-byte aligned");
-  // launch on the device that owns the workspace
+  // launch on the device that owns the workspace (the entry point's
+  // DeviceGuard puts the caller's device back)
   cudaPointerAttributes attr;
   if (cudaPointerGetAttributes(&attr, ws) == cudaSuccess && attr.type == cudaMemoryTypeDevice) {
     int cur = -1;
@@ -445,6 +584,31 @@ int ctas(int kernel) {
   const int v = g_ctas[kernel].load(std::memory_order_relaxed);
   return v > 0 ? v : kDefaultCtas[kernel];
 }
+
+// The single-frame entry points read the stream and write the planes from
+// kernels, so each must be device (or managed) memory: a host pointer is
+// rejected here instead of faulting on the GPU.
+int check_decode_pointers(const fvb_frame* frame, const uint8_t* stream, uint16_t* const* planes) {
+  if (device_of(stream) < 0) return fail(FVB_ERR_ARGUMENT, "encoded stream must be device memory");
+  for (int p = 0; p < frame->planes; ++p)
+    if (device_of(planes[p]) < 0) return fail(FVB_ERR_ARGUMENT, "output planes must be device memory");
+  return FVB_OK;
+}
+
+int check_plane_pointers(const fvb_frame* frame, const uint16_t* const* planes) {
+  for (int p = 0; p < frame->planes; ++p)
+    if (device_of(planes[p]) < 0) return fail(FVB_ERR_ARGUMENT, "input planes must be device memory");
+  return FVB_OK;
+}
+
+// Profiling records CUDA events (created on demand); the allocation-free
+// decode switches it off for its own launches.  The profiler is per thread,
+// so no other thread sees the switch.
+struct ProfilePause {
+  bool was;
+  ProfilePause() : was(g_prof.on) { g_prof.on = false; }
+  ~ProfilePause() { g_prof.on = was; }
+};
 
 std::string status_message_encode(int64_t st) {
   if (st == kStatusInternal + 1) return "tile payload is too large";
@@ -542,27 +706,52 @@ int fvb_encode_plan(int64_t width, int64_t height, int layout, int bit_depth, in
   const int rc = fill_frame(frame);
   if (rc) return rc;
   if (workspace_bytes) {
-    const Totals t = totals_of(frame, 1);
-    *workspace_bytes = static_cast<int64_t>(enc_layout(1, t).total);
+    *workspace_bytes = static_cast<int64_t>(enc_layout(totals_of(frame, 1)).total);
   }
   return FVB_OK;
 }
 
 int fvb_batch_encode_plan(const fvb_frame* frames, int n, int64_t* workspace_bytes) {
   if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
-  *workspace_bytes = static_cast<int64_t>(enc_layout(n, totals_of(frames, n)).total);
+  *workspace_bytes = static_cast<int64_t>(enc_layout(totals_of(frames, n)).total);
   return FVB_OK;
 }
 
-int fvb_batch_encode_prepare(const fvb_frame* frames, int n, const uint16_t* const* planes, const int64_t* pitches,
-                             void* workspace, int64_t workspace_bytes, void* cuda_stream) {
+int fvb_batch_bucket(const fvb_frame* frames, int n, fvb_bucket* bucket) {
+  if (n <= 0 || !frames || !bucket) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  to_bucket(bucket_of(totals_of(frames, n)), bucket);
+  return FVB_OK;
+}
+
+int fvb_bucket_encode_plan(const fvb_bucket* bucket, int64_t* workspace_bytes) {
+  Totals cap;
+  const int rc = from_bucket(bucket, &cap);
+  if (rc) return rc;
+  *workspace_bytes = static_cast<int64_t>(enc_layout(cap).total);
+  return FVB_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// ---- encoder batch internals: `cap` sizes the workspace layout and the
+// launch grids; the actual counts go to the device in BatchDims ------------
+
+int encode_prepare(const Totals& cap, const fvb_frame* frames, int n, const uint16_t* const* planes,
+                   const int64_t* pitches, void* workspace, int64_t workspace_bytes, void* cuda_stream) {
   if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
   const Totals t = totals_of(frames, n);
-  const EncLayout L = enc_layout(n, t);
+  if (!fits(t, cap)) return fail(FVB_ERR_ARGUMENT, "batch does not fit the bucket");
+  const EncLayout L = enc_layout(cap);
   int rc = check_ws(workspace, workspace_bytes, L.total);
   if (rc) return rc;
   cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
-  std::vector<FrameDesc> descs(n);
+  // one upload: the dims record, then the frame table
+  std::vector<unsigned char> table(L.frames + sizeof(FrameDesc) * n);
+  const BatchDims dims = dims_of(t);
+  std::memcpy(table.data() + L.dims, &dims, sizeof(dims));
+  FrameDesc* descs = reinterpret_cast<FrameDesc*>(table.data() + L.frames);
   const std::vector<int> order = encode_order(frames, n);
   int64_t tb = 0, sb = 0, nb = 0, pb = 0;
   for (int j = 0; j < n; ++j) {
@@ -587,21 +776,19 @@ int fvb_batch_encode_prepare(const fvb_frame* frames, int n, const uint16_t* con
     pb += d.prefix_bytes;
   }
   char* ws = static_cast<char*>(workspace);
-  FVB_CUDA(cudaMemcpyAsync(ws + L.frames, descs.data(), sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, stream));
+  FVB_CUDA(cudaMemcpyAsync(ws, table.data(), table.size(), cudaMemcpyHostToDevice, stream));
   return FVB_OK;
 }
 
-int fvb_batch_encode_enqueue(const fvb_frame* frames, int n, void* workspace, int64_t workspace_bytes,
-                             int64_t* results, void* cuda_stream) {
-  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
-  const Totals t = totals_of(frames, n);
-  const EncLayout L = enc_layout(n, t);
+int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, int64_t* results, void* cuda_stream) {
+  const EncLayout L = enc_layout(cap);
   int rc = check_ws(workspace, workspace_bytes, L.total);
   if (rc) return rc;
   rc = ensure_smem_attrs();
   if (rc) return rc;
   cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
   char* ws = static_cast<char*>(workspace);
+  const BatchDims* dims = reinterpret_cast<const BatchDims*>(ws + L.dims);
   const FrameDesc* frames_d = reinterpret_cast<const FrameDesc*>(ws + L.frames);
   FrameState* state = reinterpret_cast<FrameState*>(ws + L.state);
   int* queue = reinterpret_cast<int*>(ws + L.queue);
@@ -610,63 +797,66 @@ int fvb_batch_encode_enqueue(const fvb_frame* frames, int n, void* workspace, in
   uint8_t* rans = reinterpret_cast<uint8_t*>(ws + L.rans);
   uint8_t* prefix = reinterpret_cast<uint8_t*>(ws + L.prefix);
   uint16_t* recon = reinterpret_cast<uint16_t*>(ws + L.recon);
+  const int n = cap.frames;
   {
     LaunchScope scope_(K_ENC_INIT, stream);
-    enc_init_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, n);
+    enc_init_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, dims);
   }
   FVB_LAUNCHED("enc_init_kernel");
   // pass p covers the batch's first frames_p[p] frames (layout order)
-  for (int pass = 0; pass < t.passes; ++pass) {
-    const int nf = t.frames_p[pass];
-    const int64_t tiles = t.tiles_p[pass], nsh = t.shards_p[pass];
+  for (int pass = 0; pass < cap.passes; ++pass) {
+    const int nf = cap.frames_p[pass];
+    const int64_t tiles = cap.tiles_p[pass], nsh = cap.shards_p[pass];
     FVB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), stream));
     {
       LaunchScope scope_(K_ENC_PREDICT, stream);
       enc_predict_kernel<<<grid_for(tiles, kWarpsPerCta, ctas(K_ENC_PREDICT)), kWarpsPerCta * 32, enc_predict_smem(), stream>>>(
-          frames_d, state, nf, tiles, shards, folded, queue);
+          frames_d, state, dims, pass, shards, folded, queue);
     }
     FVB_LAUNCHED("enc_predict_kernel");
-    if (t.wide) {
+    if (cap.wide) {
       {
         LaunchScope scope_(K_ENC_PREDICT_WIDE, stream);
-        enc_predict_wide_kernel<<<grid_for(tiles, 1, ctas(K_ENC_PREDICT_WIDE)), 256, 0, stream>>>(frames_d, state, nf, tiles, folded, recon);
+        enc_predict_wide_kernel<<<grid_for(tiles, 1, ctas(K_ENC_PREDICT_WIDE)), 256, 0, stream>>>(frames_d, state, dims,
+                                                                                                  pass, folded, recon);
       }
       FVB_LAUNCHED("enc_predict_wide_kernel");
     }
     {
       // resident CTAs only: each warp streams its shards through one ring
       LaunchScope scope_(K_ENC_ANALYZE, stream);
-      enc_analyze_kernel<<<grid_for(nsh, kWarpsPerCta, ctas(K_ENC_ANALYZE)), kWarpsPerCta * 32, 0, stream>>>(frames_d, state, nf, shards,
-                                                                                           nsh, folded, rans);
+      enc_analyze_kernel<<<grid_for(nsh, kWarpsPerCta, ctas(K_ENC_ANALYZE)), kWarpsPerCta * 32, 0, stream>>>(
+          frames_d, state, dims, pass, shards, folded, rans);
     }
     FVB_LAUNCHED("enc_analyze_kernel");
     {
       LaunchScope scope_(K_ENC_RANS, stream);
       enc_rans_kernel<<<static_cast<int>(ceil_div(nsh * 4 > 0 ? nsh * 4 : 1, 128)), 128, 0, stream>>>(
-          state, shards, nsh, folded, rans);
+          state, dims, pass, shards, folded, rans);
     }
     FVB_LAUNCHED("enc_rans_kernel");
     {
       LaunchScope scope_(K_ENC_SCAN, stream);
-      enc_scan_kernel<<<nf, 1024, 0, stream>>>(frames_d, state, nf, shards, prefix);
+      enc_scan_kernel<<<nf > 0 ? nf : 1, 1024, 0, stream>>>(frames_d, state, dims, pass, shards, prefix);
     }
     FVB_LAUNCHED("enc_scan_kernel");
   }
   int64_t* res_d = reinterpret_cast<int64_t*>(ws + L.results);
   {
     LaunchScope scope_(K_RESULTS, stream);
-    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, n, res_d, 0);
+    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, dims, res_d, 0);
   }
   FVB_LAUNCHED("results_kernel");
   if (results) FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
   return FVB_OK;
 }
 
-int fvb_batch_encode_emit(const fvb_frame* frames, int n, void* workspace, int64_t workspace_bytes,
-                          uint8_t* const* outs, void* cuda_stream) {
+int encode_emit(const Totals& cap, const fvb_frame* frames, int n, void* workspace, int64_t workspace_bytes,
+                uint8_t* const* outs, void* cuda_stream) {
   if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
   const Totals t = totals_of(frames, n);
-  const EncLayout L = enc_layout(n, t);
+  if (!fits(t, cap)) return fail(FVB_ERR_ARGUMENT, "batch does not fit the bucket");
+  const EncLayout L = enc_layout(cap);
   int rc = check_ws(workspace, workspace_bytes, L.total);
   if (rc) return rc;
   rc = ensure_smem_attrs();
@@ -699,12 +889,67 @@ int fvb_batch_encode_emit(const fvb_frame* frames, int n, void* workspace, int64
   return FVB_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int fvb_batch_encode_prepare(const fvb_frame* frames, int n, const uint16_t* const* planes, const int64_t* pitches,
+                             void* workspace, int64_t workspace_bytes, void* cuda_stream) {
+  DeviceGuard guard_;
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  return encode_prepare(totals_of(frames, n), frames, n, planes, pitches, workspace, workspace_bytes, cuda_stream);
+}
+
+int fvb_batch_encode_enqueue(const fvb_frame* frames, int n, void* workspace, int64_t workspace_bytes,
+                             int64_t* results, void* cuda_stream) {
+  DeviceGuard guard_;
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  return encode_enqueue(totals_of(frames, n), workspace, workspace_bytes, results, cuda_stream);
+}
+
+int fvb_batch_encode_emit(const fvb_frame* frames, int n, void* workspace, int64_t workspace_bytes,
+                          uint8_t* const* outs, void* cuda_stream) {
+  DeviceGuard guard_;
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  return encode_emit(totals_of(frames, n), frames, n, workspace, workspace_bytes, outs, cuda_stream);
+}
+
+int fvb_bucket_encode_prepare(const fvb_bucket* bucket, const fvb_frame* frames, int n, const uint16_t* const* planes,
+                              const int64_t* pitches, void* workspace, int64_t workspace_bytes, void* cuda_stream) {
+  DeviceGuard guard_;
+  Totals cap;
+  const int rc = from_bucket(bucket, &cap);
+  if (rc) return rc;
+  return encode_prepare(cap, frames, n, planes, pitches, workspace, workspace_bytes, cuda_stream);
+}
+
+int fvb_bucket_encode_enqueue(const fvb_bucket* bucket, void* workspace, int64_t workspace_bytes, int64_t* results,
+                              void* cuda_stream) {
+  DeviceGuard guard_;
+  Totals cap;
+  const int rc = from_bucket(bucket, &cap);
+  if (rc) return rc;
+  return encode_enqueue(cap, workspace, workspace_bytes, results, cuda_stream);
+}
+
+int fvb_bucket_encode_emit(const fvb_bucket* bucket, const fvb_frame* frames, int n, void* workspace,
+                           int64_t workspace_bytes, uint8_t* const* outs, void* cuda_stream) {
+  DeviceGuard guard_;
+  Totals cap;
+  const int rc = from_bucket(bucket, &cap);
+  if (rc) return rc;
+  return encode_emit(cap, frames, n, workspace, workspace_bytes, outs, cuda_stream);
+}
+
 int fvb_encode_analyze(const fvb_frame* frame, const uint16_t* const* planes, const int64_t* pitches, void* workspace,
                        int64_t workspace_bytes, void* cuda_stream, int64_t* stream_len) {
-  if (!frame) return fail(FVB_ERR_ARGUMENT, "frame is null");
+  DeviceGuard guard_;
+  if (!frame || !planes || !pitches) return fail(FVB_ERR_ARGUMENT, "null argument");
+  int rc = check_plane_pointers(frame, planes);
+  if (rc) return rc;
   const uint16_t* p3[3] = {planes[0], frame->planes == 3 ? planes[1] : nullptr, frame->planes == 3 ? planes[2] : nullptr};
   const int64_t q3[3] = {pitches[0], frame->planes == 3 ? pitches[1] : 0, frame->planes == 3 ? pitches[2] : 0};
-  int rc = fvb_batch_encode_prepare(frame, 1, p3, q3, workspace, workspace_bytes, cuda_stream);
+  rc = fvb_batch_encode_prepare(frame, 1, p3, q3, workspace, workspace_bytes, cuda_stream);
   if (rc) return rc;
   int64_t res[2] = {0, 0};
   rc = fvb_batch_encode_enqueue(frame, 1, workspace, workspace_bytes, res, cuda_stream);
@@ -718,6 +963,7 @@ int fvb_encode_analyze(const fvb_frame* frame, const uint16_t* const* planes, co
 
 int fvb_encode_emit(const fvb_frame* frame, void* workspace, int64_t workspace_bytes, uint8_t* out, int64_t out_len,
                     void* cuda_stream) {
+  DeviceGuard guard_;
   if (!frame || !out) return fail(FVB_ERR_ARGUMENT, "null argument");
   (void)out_len;
   uint8_t* outs[1] = {out};
@@ -773,12 +1019,13 @@ int fvb_decode_plan(const uint8_t* b, int64_t header_len, int64_t size, fvb_fram
   frame->step = refined ? refined_gray16_step(quality) : quantization_step(layout, depth, quality);
   int rc = fill_frame(frame);
   if (rc) return rc;
-  if (workspace_bytes) *workspace_bytes = static_cast<int64_t>(dec_layout(1, totals_of(frame, 1)).total);
+  if (workspace_bytes) *workspace_bytes = static_cast<int64_t>(dec_layout(totals_of(frame, 1)).total);
   return FVB_OK;
 }
 
 int fvb_gather_headers(const uint8_t* const* streams, const int64_t* stream_lens, int n, void* scratch,
                        int64_t scratch_bytes, uint8_t* headers, void* cuda_stream) {
+  DeviceGuard guard_;
   if (n <= 0 || !streams || !headers) return fail(FVB_ERR_ARGUMENT, "empty batch");
   const size_t need = align_up(16 * static_cast<size_t>(n)) + kHeaderBytes * static_cast<size_t>(n);
   int rc = check_ws(scratch, scratch_bytes, need);
@@ -806,24 +1053,15 @@ int fvb_gather_headers(const uint8_t* const* streams, const int64_t* stream_lens
 
 int fvb_batch_decode_plan(const fvb_frame* frames, int n, int64_t* workspace_bytes) {
   if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
-  *workspace_bytes = static_cast<int64_t>(dec_layout(n, totals_of(frames, n)).total);
+  *workspace_bytes = static_cast<int64_t>(dec_layout(totals_of(frames, n)).total);
   return FVB_OK;
 }
 
-int fvb_batch_decode_prepare(const fvb_frame* frames, int n, const uint8_t* const* streams, const int64_t* stream_lens,
-                             uint16_t* const* planes, const int64_t* pitches, void* workspace, int64_t workspace_bytes,
-                             void* cuda_stream) {
-  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
-  const Totals t = totals_of(frames, n);
-  const DecLayout L = dec_layout(n, t);
-  int rc = check_ws(workspace, workspace_bytes, L.total);
+int fvb_bucket_decode_plan(const fvb_bucket* bucket, int64_t* workspace_bytes) {
+  Totals cap;
+  const int rc = from_bucket(bucket, &cap);
   if (rc) return rc;
-  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
-  std::vector<FrameDesc> descs(n);
-  rc = fill_decode_descs(frames, n, streams, stream_lens, planes, pitches, descs.data());
-  if (rc) return rc;
-  char* ws = static_cast<char*>(workspace);
-  FVB_CUDA(cudaMemcpyAsync(ws + L.frames, descs.data(), sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, stream));
+  *workspace_bytes = static_cast<int64_t>(dec_layout(cap).total);
   return FVB_OK;
 }
 
@@ -859,21 +1097,42 @@ int fill_decode_descs(const fvb_frame* frames, int n, const uint8_t* const* stre
   return FVB_OK;
 }
 
-}  // namespace
 
-extern "C" {
-
-int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void* workspace, int64_t workspace_bytes,
-                             int64_t* results, void* cuda_stream) {
+int decode_prepare(const Totals& cap, const fvb_frame* frames, int n, const uint8_t* const* streams,
+                   const int64_t* stream_lens, uint16_t* const* planes, const int64_t* pitches, void* workspace,
+                   int64_t workspace_bytes, void* cuda_stream) {
   if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
   const Totals t = totals_of(frames, n);
-  const DecLayout L = dec_layout(n, t);
+  if (!fits(t, cap)) return fail(FVB_ERR_ARGUMENT, "batch does not fit the bucket");
+  const DecLayout L = dec_layout(cap);
+  int rc = check_ws(workspace, workspace_bytes, L.total);
+  if (rc) return rc;
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  // one upload: the dims record, then the frame table
+  std::vector<unsigned char> table(L.frames + sizeof(FrameDesc) * n);
+  const BatchDims dims = dims_of(t);
+  std::memcpy(table.data() + L.dims, &dims, sizeof(dims));
+  rc = fill_decode_descs(frames, n, streams, stream_lens, planes, pitches,
+                         reinterpret_cast<FrameDesc*>(table.data() + L.frames));
+  if (rc) return rc;
+  FVB_CUDA(cudaMemcpyAsync(workspace, table.data(), table.size(), cudaMemcpyHostToDevice, stream));
+  return FVB_OK;
+}
+
+// The decode launch sequence.  `side_ok`: large batches may run dec_other on
+// the calling thread's side stream (created on first use); the
+// allocation-free decode passes false, so it never creates a stream.
+int decode_enqueue(const Totals& t, int wavefront, void* workspace, int64_t workspace_bytes, int64_t* results,
+                   void* cuda_stream, bool side_ok) {
+  const int n = t.frames;
+  const DecLayout L = dec_layout(t);
   int rc = check_ws(workspace, workspace_bytes, L.total);
   if (rc) return rc;
   rc = ensure_smem_attrs();
   if (rc) return rc;
   cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
   char* ws = static_cast<char*>(workspace);
+  const BatchDims* dims = reinterpret_cast<const BatchDims*>(ws + L.dims);
   const FrameDesc* frames_d = reinterpret_cast<const FrameDesc*>(ws + L.frames);
   FrameState* state = reinterpret_cast<FrameState*>(ws + L.state);
   int* queue = reinterpret_cast<int*>(ws + L.queue);
@@ -886,8 +1145,8 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
   FVB_CUDA(cudaMemsetAsync(lists, 0, sizeof(DecodeLists), stream));
   {
     LaunchScope scope_(K_DEC_PARSE, stream);
-    dec_parse_kernel<<<grid_for(t.tiles, 128, ctas(K_DEC_PARSE)), 128, 0, stream>>>(frames_d, state, n, t.tiles, shards, t.shards,
-                                                                       lists, items);
+    dec_parse_kernel<<<grid_for(t.tiles, 128, ctas(K_DEC_PARSE)), 128, 0, stream>>>(frames_d, state, dims, shards, lists,
+                                                                                      items);
   }
   FVB_LAUNCHED("dec_parse_kernel");
   RansTable* tables = reinterpret_cast<RansTable*>(ws + L.tables);
@@ -898,7 +1157,7 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
   }
   FVB_LAUNCHED("dec_rans_tables_kernel");
   SideStream* side = nullptr;
-  if (t.shards >= kSideStreamShards) {
+  if (side_ok && t.shards >= kSideStreamShards) {
     rc = side_stream(&side);
     if (rc) return rc;
   }
@@ -917,7 +1176,7 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
     {
       LaunchScope scope_(K_DEC_OTHER, other);
       dec_other_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), 4, ctas(K_DEC_OTHER)), 128, 0, other>>>(
-          frames_d, state, shards, t.shards, lists, items, folded);
+          frames_d, state, shards, dims, lists, items, folded);
     }
     const cudaError_t launched = cudaGetLastError();
     if (side) {  // joined even when the launch failed, so a stream capture is never left forked
@@ -930,42 +1189,86 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
     {
       LaunchScope scope_(K_DEC_RECON, stream);
       dec_reconstruct_kernel<<<grid_for(t.tiles, kWarpsPerCta, ctas(K_DEC_RECON)), kWarpsPerCta * 32, dec_reconstruct_smem(), stream>>>(
-          frames_d, state, n, t.tiles, folded, queue);
+          frames_d, state, dims, folded, queue);
     }
     FVB_LAUNCHED("dec_reconstruct_kernel");
     if (t.wide) {
       {
         LaunchScope scope_(K_DEC_RECON_WIDE, stream);
-        dec_reconstruct_wide_kernel<<<grid_for(t.tiles, 1, ctas(K_DEC_RECON_WIDE)), 256, 0, stream>>>(frames_d, state, n, t.tiles, folded);
+        dec_reconstruct_wide_kernel<<<grid_for(t.tiles, 1, ctas(K_DEC_RECON_WIDE)), 256, 0, stream>>>(frames_d, state, dims, folded);
       }
       FVB_LAUNCHED("dec_reconstruct_wide_kernel");
     }
   } else {
     {
       LaunchScope scope_(K_DEC_RECON_SERIAL, stream);
-      dec_reconstruct_serial_kernel<<<static_cast<int>(ceil_div(t.tiles, 128)), 128, 0, stream>>>(frames_d, state, n,
-                                                                                                 t.tiles, folded);
+      dec_reconstruct_serial_kernel<<<static_cast<int>(ceil_div(t.tiles, 128)), 128, 0, stream>>>(frames_d, state, dims,
+                                                                                                 folded);
     }
     FVB_LAUNCHED("dec_reconstruct_serial_kernel");
   }
   int64_t* res_d = reinterpret_cast<int64_t*>(ws + L.results);
   {
     LaunchScope scope_(K_RESULTS, stream);
-    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, n, res_d, 1);
+    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, dims, res_d, 1);
   }
   FVB_LAUNCHED("results_kernel");
   if (results) FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
   return FVB_OK;
 }
 
+
+}  // namespace
+
+extern "C" {
+
+int fvb_batch_decode_prepare(const fvb_frame* frames, int n, const uint8_t* const* streams, const int64_t* stream_lens,
+                             uint16_t* const* planes, const int64_t* pitches, void* workspace, int64_t workspace_bytes,
+                             void* cuda_stream) {
+  DeviceGuard guard_;
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  return decode_prepare(totals_of(frames, n), frames, n, streams, stream_lens, planes, pitches, workspace,
+                        workspace_bytes, cuda_stream);
+}
+
+int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void* workspace, int64_t workspace_bytes,
+                             int64_t* results, void* cuda_stream) {
+  DeviceGuard guard_;
+  if (n <= 0 || !frames) return fail(FVB_ERR_ARGUMENT, "empty batch");
+  return decode_enqueue(totals_of(frames, n), wavefront, workspace, workspace_bytes, results, cuda_stream, true);
+}
+
+int fvb_bucket_decode_prepare(const fvb_bucket* bucket, const fvb_frame* frames, int n, const uint8_t* const* streams,
+                              const int64_t* stream_lens, uint16_t* const* planes, const int64_t* pitches,
+                              void* workspace, int64_t workspace_bytes, void* cuda_stream) {
+  DeviceGuard guard_;
+  Totals cap;
+  const int rc = from_bucket(bucket, &cap);
+  if (rc) return rc;
+  return decode_prepare(cap, frames, n, streams, stream_lens, planes, pitches, workspace, workspace_bytes,
+                        cuda_stream);
+}
+
+int fvb_bucket_decode_enqueue(const fvb_bucket* bucket, int wavefront, void* workspace, int64_t workspace_bytes,
+                              int64_t* results, void* cuda_stream) {
+  DeviceGuard guard_;
+  Totals cap;
+  const int rc = from_bucket(bucket, &cap);
+  if (rc) return rc;
+  return decode_enqueue(cap, wavefront, workspace, workspace_bytes, results, cuda_stream, true);
+}
+
 int fvb_decode(const fvb_frame* frame, const uint8_t* stream, int64_t stream_len, uint16_t* const* planes,
                const int64_t* pitches, int wavefront, void* workspace, int64_t workspace_bytes, void* cuda_stream) {
-  if (!frame) return fail(FVB_ERR_ARGUMENT, "frame is null");
+  DeviceGuard guard_;
+  if (!frame || !planes || !pitches) return fail(FVB_ERR_ARGUMENT, "null argument");
+  int rc = check_decode_pointers(frame, stream, planes);
+  if (rc) return rc;
   uint16_t* p3[3] = {planes[0], frame->planes == 3 ? planes[1] : nullptr, frame->planes == 3 ? planes[2] : nullptr};
   const int64_t q3[3] = {pitches[0], frame->planes == 3 ? pitches[1] : 0, frame->planes == 3 ? pitches[2] : 0};
   const uint8_t* s1[1] = {stream};
   const int64_t l1[1] = {stream_len};
-  int rc = fvb_batch_decode_prepare(frame, 1, s1, l1, p3, q3, workspace, workspace_bytes, cuda_stream);
+  rc = fvb_batch_decode_prepare(frame, 1, s1, l1, p3, q3, workspace, workspace_bytes, cuda_stream);
   if (rc) return rc;
   int64_t res[2] = {0, 0};
   rc = fvb_batch_decode_enqueue(frame, 1, wavefront, workspace, workspace_bytes, res, cuda_stream);
@@ -1013,9 +1316,13 @@ int noalloc_scratch(int device, void** out) {
     FVB_CUDA(cudaGetDevice(&cur));
     if (cur != device) FVB_CUDA(cudaSetDevice(device));
     void* ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    // the kernels' shared-memory limits are set here too, so that later calls
+    // only launch
+    const int attrs = e == cudaSuccess ? ensure_smem_attrs() : FVB_OK;
     if (cur != device) cudaSetDevice(cur);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    if (attrs) return attrs;
     g_noalloc_address[device] = ptr;
   }
   *out = g_noalloc_address[device];
@@ -1030,9 +1337,10 @@ int64_t fvb_decode_noalloc_capacity(void) { return static_cast<int64_t>(kNoAlloc
 
 int fvb_decode_noalloc(const fvb_frame* frame, const uint8_t* stream, int64_t stream_len, uint16_t* const* planes,
                        const int64_t* pitches, int wavefront, void* cuda_stream) {
+  DeviceGuard guard_;
   if (!frame || !stream || !planes || !pitches) return fail(FVB_ERR_ARGUMENT, "null argument");
   const Totals t = totals_of(frame, 1);
-  const DecLayout L = dec_layout(1, t);
+  const DecLayout L = dec_layout(t);
   if (L.total > kNoAllocScratchBytes) {
     char buf[192];
     std::snprintf(buf, sizeof(buf),
@@ -1041,17 +1349,13 @@ int fvb_decode_noalloc(const fvb_frame* frame, const uint8_t* stream, int64_t st
                   L.total, kNoAllocScratchBytes);
     return fail(FVB_ERR_WORKSPACE, buf);
   }
-  // the device that holds the output planes does the work
-  cudaPointerAttributes attr;
-  if (cudaPointerGetAttributes(&attr, planes[0]) != cudaSuccess || attr.type != cudaMemoryTypeDevice) {
-    cudaGetLastError();
-    return fail(FVB_ERR_ARGUMENT, "output planes must be device memory");
-  }
-  void* scratch = nullptr;
-  int rc = noalloc_scratch(attr.device, &scratch);
+  int rc = check_decode_pointers(frame, stream, planes);
   if (rc) return rc;
-  const bool profiling = g_prof.on;  // profiling would create CUDA events
-  g_prof.on = false;
+  // the device that holds the output planes does the work
+  void* scratch = nullptr;
+  rc = noalloc_scratch(device_of(planes[0]), &scratch);
+  if (rc) return rc;
+  const ProfilePause no_events;
   uint16_t* p3[3] = {planes[0], frame->planes == 3 ? planes[1] : nullptr, frame->planes == 3 ? planes[2] : nullptr};
   const int64_t q3[3] = {pitches[0], frame->planes == 3 ? pitches[1] : 0, frame->planes == 3 ? pitches[2] : 0};
   const uint8_t* s1[1] = {stream};
@@ -1060,15 +1364,16 @@ int fvb_decode_noalloc(const fvb_frame* frame, const uint8_t* stream, int64_t st
   int64_t res[2] = {0, 0};
   FrameDesc desc;
   rc = check_ws(scratch, static_cast<int64_t>(kNoAllocScratchBytes), L.total);
-  if (!rc) rc = fill_decode_descs(frame, 1, s1, l1, p3, q3, &desc);
-  if (!rc) {
-    const cudaError_t e = cudaMemcpyAsync(static_cast<char*>(scratch) + L.frames, &desc, sizeof(FrameDesc),
-                                          cudaMemcpyHostToDevice, cs);
-    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(frame descriptor)");
-  }
-  if (!rc) rc = fvb_batch_decode_enqueue(frame, 1, wavefront, scratch, static_cast<int64_t>(kNoAllocScratchBytes),
-                                         res, cuda_stream);
-  g_prof.on = profiling;
+  if (rc) return rc;
+  rc = fill_decode_descs(frame, 1, s1, l1, p3, q3, &desc);
+  if (rc) return rc;
+  const BatchDims dims = dims_of(t);
+  FVB_CUDA(cudaMemcpyAsync(static_cast<char*>(scratch) + L.dims, &dims, sizeof(BatchDims), cudaMemcpyHostToDevice,
+                           cs));
+  FVB_CUDA(cudaMemcpyAsync(static_cast<char*>(scratch) + L.frames, &desc, sizeof(FrameDesc), cudaMemcpyHostToDevice,
+                           cs));
+  // no side stream: dec_other runs on the caller's stream, so nothing is created
+  rc = decode_enqueue(t, wavefront, scratch, static_cast<int64_t>(kNoAllocScratchBytes), res, cuda_stream, false);
   if (rc) return rc;
   FVB_CUDA(cudaStreamSynchronize(cs));
   if (res[0] != 0) {

@@ -83,6 +83,21 @@ struct FrameDesc {
   uint32_t fps_num, fps_den;
 };
 
+// Counts of the work of one batch, read by the kernels from device memory
+// (written with the frame table), so that a launch sequence captured for a
+// bucket of batch sizes -- grids sized for the bucket's capacity -- serves
+// any batch that fits it.  frames_p / tiles_p / shards_p: the frames, tiles
+// and shards that take part in encoder pass p (the batch is laid out with
+// frames of more passes first, so these are prefixes); entry 0 counts the
+// whole batch (decode uses entry 0 only).
+struct BatchDims {
+  int32_t frames_p[3];
+  int32_t passes;
+  int64_t tiles_p[3];
+  int64_t shards_p[3];
+  int64_t samples;
+};
+
 // Per-frame mutable state (device), one per frame of a batch.
 struct FrameState {
   int32_t step;        // step of the current pass

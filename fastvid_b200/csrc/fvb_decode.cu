@@ -45,9 +45,11 @@ __device__ __forceinline__ int list_of_mode(int mode) {
 // dec_parse: directory entry checks (status 10) and shard header walk
 // (status 11), one thread per tile.
 
-__global__ void dec_parse_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state, int nframes,
-                                 int64_t total_tiles, ShardInfo* __restrict__ shards, int64_t total_shards,
+__global__ void dec_parse_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
+                                 const BatchDims* __restrict__ dims, ShardInfo* __restrict__ shards,
                                  DecodeLists* __restrict__ lists, int32_t* __restrict__ list_items) {
+  const int nframes = dims->frames_p[0];
+  const int64_t total_tiles = dims->tiles_p[0], total_shards = dims->shards_p[0];
   for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total_tiles;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int fi = frame_of_tile(frames, nframes, t);
@@ -232,21 +234,27 @@ struct ByteWindow {
 };
 
 
-// A lane's byte stream through a private ring of 32 words in shared memory,
-// fed by cp.async: 24 words before the first read, then two words with every
+// A lane's byte stream through a private ring of 16 words in shared memory,
+// fed by cp.async: 12 words before the first read, then two words with every
 // eight-byte read -- as many as four decoding steps can consume -- so the
-// ring stays at least 24 words ahead of the read position, and a read, which
-// may leave the newest four copy groups in flight, only touches words copied
-// long before.  There is no refill branch: every read issues its two copies
-// under predicates.  Word w of the aligned range lives in slot w % 32; slot s
-// of lane l is word s * 32 + l of the warp's ring block, so every lane reads
-// and fills its own bank whatever its position.  Only words holding a byte of
-// the lane are copied (others keep stale bytes, and reading them is an
-// overrun that the byte count check reports).
+// ring stays at least 12 words ahead of the read position (the gap shrinks by
+// at most the two words a read consumes and grows by the two it issues, up
+// to the ring size).  A read may leave the newest four copy groups in flight;
+// the words it touches (w .. w+2, at most ten words below the copy front,
+// which advances at most two words per read) were issued five or more reads
+// earlier, so their groups are complete.  There is no refill branch: every
+// read issues its two copies under predicates.  Word w of the aligned range
+// lives in slot w % 16; slot s of lane l is word s * 32 + l of the warp's ring
+// block, so every lane reads and fills its own bank whatever its position.
+// Only words holding a byte of the lane are copied (others keep stale bytes,
+// and reading them is an overrun that the byte count check reports).  A
+// 16-word ring (2 KB per warp, 32 before) lets four dec_rans CTAs share an
+// SM.
 struct LaneRing {
-  static constexpr int kWords = 32;    // slots per lane
-  static constexpr int kFill = 24;     // words copied before the first read
+  static constexpr int kWords = 16;    // slots per lane
+  static constexpr int kFill = 12;     // words copied before the first read
   static constexpr int kInFlight = 4;  // copy groups a read may leave pending
+  static_assert(kFill >= 10 && kFill <= kWords, "read words must be five copy groups old");
   uint32_t* ring;          // slot 0 of this lane (slots 32 words apart)
   const uint32_t* words;   // aligned base of the lane's bytes
   int head;                // lane byte 0 = byte `head` of word 0
@@ -548,8 +556,10 @@ struct OtherGroupSm {
 
 __global__ void __launch_bounds__(128)
 dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
-                 const ShardInfo* __restrict__ shards, int64_t total_shards, DecodeLists* __restrict__ lists,
-                 const int32_t* __restrict__ list_items, uint32_t* __restrict__ folded) {
+                 const ShardInfo* __restrict__ shards, const BatchDims* __restrict__ dims,
+                 DecodeLists* __restrict__ lists, const int32_t* __restrict__ list_items,
+                 uint32_t* __restrict__ folded) {
+  const int64_t total_shards = dims->shards_p[0];
   __shared__ OtherGroupSm sm_all[4];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   OtherGroupSm& sm = sm_all[warp];
@@ -905,8 +915,11 @@ __device__ void rec_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
 }
 
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
-dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state, int nframes,
-                       int64_t total_tiles, const uint32_t* __restrict__ folded, int* __restrict__ queue) {
+dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
+                       const BatchDims* __restrict__ dims, const uint32_t* __restrict__ folded,
+                       int* __restrict__ queue) {
+  const int nframes = dims->frames_p[0];
+  const int64_t total_tiles = dims->tiles_p[0];
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   RecWarpSmem& sm = reinterpret_cast<RecWarpSmem*>(smem_raw)[warp];
@@ -934,7 +947,9 @@ dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* _
 // Wide tiles: antidiagonal order with neighbours read back from the output
 // plane (decode.cu:572-605).
 __global__ void dec_reconstruct_wide_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
-                                            int nframes, int64_t total_tiles, const uint32_t* __restrict__ folded) {
+                                            const BatchDims* __restrict__ dims, const uint32_t* __restrict__ folded) {
+  const int nframes = dims->frames_p[0];
+  const int64_t total_tiles = dims->tiles_p[0];
   for (int64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
     const int fi = frame_of_tile(frames, nframes, t);
     const FrameDesc& f = frames[fi];
@@ -963,7 +978,9 @@ __global__ void dec_reconstruct_wide_kernel(const FrameDesc* __restrict__ frames
 
 // predictor="serial": one thread per tile in raster order (decode.cu:608-656).
 __global__ void dec_reconstruct_serial_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
-                                              int nframes, int64_t total_tiles, const uint32_t* __restrict__ folded) {
+                                              const BatchDims* __restrict__ dims, const uint32_t* __restrict__ folded) {
+  const int nframes = dims->frames_p[0];
+  const int64_t total_tiles = dims->tiles_p[0];
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= total_tiles) return;
   const int fi = frame_of_tile(frames, nframes, t);

@@ -168,10 +168,12 @@ __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
 }
 
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
-enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state, int nframes,
-                   int64_t total_tiles, ShardInfo* __restrict__ shards, uint32_t* __restrict__ folded,
-                   int* __restrict__ queue) {
+enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
+                   const BatchDims* __restrict__ dims, int pass, ShardInfo* __restrict__ shards,
+                   uint32_t* __restrict__ folded, int* __restrict__ queue) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nframes = dims->frames_p[pass];
+  const int64_t total_tiles = dims->tiles_p[pass];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   EncWarpSmem& sm = reinterpret_cast<EncWarpSmem*>(smem_raw)[warp];
   for (;;) {
@@ -213,8 +215,10 @@ enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
 // the reconstruction kept in global scratch (same order as the reference,
 // encode.cu:150-192).  Only used for unusually wide tile sizes.
 __global__ void enc_predict_wide_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
-                                        int nframes, int64_t total_tiles, uint32_t* __restrict__ folded,
+                                        const BatchDims* __restrict__ dims, int pass, uint32_t* __restrict__ folded,
                                         uint16_t* __restrict__ recon) {
+  const int nframes = dims->frames_p[pass];
+  const int64_t total_tiles = dims->tiles_p[pass];
   for (int64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
     const int fi = frame_of_tile(frames, nframes, t);
     const FrameDesc& f = frames[fi];
@@ -335,9 +339,11 @@ __device__ __forceinline__ void run_block(RunStats& r, uint32_t zm, int32_t p0, 
 }
 
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 6)
-enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state, int nframes,
-                   ShardInfo* __restrict__ shards, int64_t total_shards,
+enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
+                   const BatchDims* __restrict__ dims, int pass, ShardInfo* __restrict__ shards,
                    const uint32_t* __restrict__ folded, uint8_t* __restrict__ rans_scratch) {
+  const int nframes = dims->frames_p[pass];
+  const int64_t total_shards = dims->shards_p[pass];
   // Class counts: two classes share a 32-bit word (16-bit counts: a class
   // holds at most 1024 symbols); the words of classes (0,1) and (2,3) of a
   // value sit 520 words apart, in different banks.  list: the present values
@@ -792,8 +798,10 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
 // stream order (the reference reverses them at emission, encode.cu:609).
 
 __global__ void __launch_bounds__(128)
-enc_rans_kernel(const FrameState* __restrict__ state, ShardInfo* __restrict__ shards, int64_t total_shards,
-                const uint32_t* __restrict__ folded, uint8_t* __restrict__ rans_scratch) {
+enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restrict__ dims, int pass,
+                ShardInfo* __restrict__ shards, const uint32_t* __restrict__ folded,
+                uint8_t* __restrict__ rans_scratch) {
+  const int64_t total_shards = dims->shards_p[pass];
   const int64_t gid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t s = gid >> 2;
   const int lane = static_cast<int>(gid & 3);
@@ -861,8 +869,10 @@ __device__ __forceinline__ void put32(uint8_t* p, uint32_t v) {
 }
 
 __global__ void __launch_bounds__(1024)
-enc_scan_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state, int nframes,
-                ShardInfo* __restrict__ shards, uint8_t* __restrict__ prefix) {
+enc_scan_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
+                const BatchDims* __restrict__ dims, int pass, ShardInfo* __restrict__ shards,
+                uint8_t* __restrict__ prefix) {
+  const int nframes = dims->frames_p[pass];
   __shared__ int64_t warp_tot[32];
   __shared__ int64_t carry_s;
   const int fi = blockIdx.x;
@@ -1012,7 +1022,9 @@ enc_scan_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
 
 // Reset per-pass state before the first pass (device side, so batches need
 // no host writes).
-__global__ void enc_init_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state, int nframes) {
+__global__ void enc_init_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
+                                const BatchDims* __restrict__ dims) {
+  const int nframes = dims->frames_p[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nframes) return;
   FrameState s{};
@@ -1031,15 +1043,18 @@ __global__ void enc_init_kernel(const FrameDesc* __restrict__ frames, FrameState
 // atomics, so no global atomics and no pre-zeroed output -- and copied out
 // with aligned 32-bit stores plus byte stores at the two ragged ends.
 
+// record buffer words: the largest record plus slack, rounded up to whole
+// 16-byte vectors (so every warp's buffer is 16-byte aligned and is cleared
+// with vector stores)
+constexpr int kEmitWords = ((kMaxRecordBytes + 8 + 3) / 4 + 3) & ~3;
+
 struct EmitWarpSmem {
-  uint32_t buf[(kMaxRecordBytes + 8 + 3) / 4];
+  uint32_t buf[kEmitWords];
 };
-static_assert(sizeof(EmitWarpSmem) % 16 == 0 || true, "");
+static_assert(sizeof(EmitWarpSmem) % 16 == 0, "record buffers must stay 16-byte aligned");
 
 size_t enc_predict_smem() { return sizeof(EncWarpSmem) * kWarpsPerCta; }
 size_t enc_emit_smem() { return sizeof(EmitWarpSmem) * kWarpsPerCta; }
-
-constexpr int kEmitWords = (kMaxRecordBytes + 8 + 3) / 4;
 
 // Every write into the record buffer is bounds-checked: a record can never
 // outgrow kMaxRecordBytes, and a write past it is dropped rather than
@@ -1057,29 +1072,64 @@ __device__ __forceinline__ void put_byte(uint32_t* buf, int pos, uint32_t byte) 
   atomicOr(&buf[pos >> 2], (byte & 0xffu) << ((pos & 3) * 8));
 }
 
-// Record bytes [pos, pos+len) <- src[0, len) (global, any alignment), four
-// bytes per lane and step: record word d takes source bytes 4d-pos .. +3,
-// gathered from the two aligned source words that hold them (only words
-// holding a byte of the piece are read) and merged with one shared atomic,
-// the bytes outside the piece masked off.
+// Record bytes [pos, pos+len) <- src[0, len) (global, any alignment).  Record
+// word d (bytes 4d .. 4d+3) takes source bytes 4d-pos .. 4d-pos+3: the funnel
+// shift of the two aligned source words that hold them, by the same amount
+// for every d.  Each lane loads one source word; the word above it comes from
+// the next lane (lane 31 loads its own), and the loads of two rounds of 32
+// words are issued before either round is merged.  Words wholly inside the
+// piece are plain stores; the two end words, which neighbouring pieces share,
+// are merged with a shared atomic.  Only source words holding a byte of the
+// piece are read.
 __device__ __forceinline__ void put_bytes(uint32_t* buf, int pos, const uint8_t* __restrict__ src, int len, int lane) {
   if (len <= 0) return;
   const uintptr_t sa = reinterpret_cast<uintptr_t>(src);
   const uint32_t* __restrict__ sw = reinterpret_cast<const uint32_t*>(sa & ~static_cast<uintptr_t>(3));
   const int h = static_cast<int>(sa & 3);
   const int last_w = (h + len - 1) >> 2;  // last source word holding a piece byte
+  const int qb = h - pos;                 // source byte index of record byte 4d is qb + 4d (>= -3)
+  const int sh = 8 * (qb & 3);
+  const int d0 = pos >> 2;
   const int d1 = min((pos + len - 1) >> 2, kEmitWords - 1);
-  for (int d = (pos >> 2) + lane; d <= d1; d += 32) {
-    const int s0 = 4 * d - pos;  // piece offset of record byte 4d (>= -3)
-    const int q = h + s0;        // its byte index from sw (>= -3)
-    const int wi = q >> 2;       // floor: -1 for q in -3..-1
-    const uint32_t lo = wi >= 0 ? __ldg(sw + wi) : 0u;
-    const uint32_t hi = wi + 1 <= last_w ? __ldg(sw + wi + 1) : 0u;
-    const uint32_t v = __funnelshift_r(lo, hi, 8 * (q & 3));
-    const int k0 = max(0, -s0), k1 = min(3, len - 1 - s0);
-    const uint32_t mask = (0xffffffffu >> (8 * (3 - k1))) & (0xffffffffu << (8 * k0));
-    atomicOr(&buf[d], v & mask);
+  auto word = [&](int wi) { return (wi >= 0 && wi <= last_w) ? __ldg(sw + wi) : 0u; };
+  for (int dd = d0; dd <= d1; dd += 64) {
+    const int da = dd + lane, db = dd + 32 + lane;
+    const int wa = (qb + 4 * da) >> 2, wb = (qb + 4 * db) >> 2;  // floor
+    const uint32_t la = word(wa);
+    const uint32_t lb = dd + 32 <= d1 ? word(wb) : 0u;
+    const uint32_t ta = lane == 31 ? word(wa + 1) : 0u;
+    const uint32_t tb = (lane == 31 && dd + 32 <= d1) ? word(wb + 1) : 0u;
+    uint32_t ha = __shfl_down_sync(0xffffffffu, la, 1);
+    uint32_t hb = __shfl_down_sync(0xffffffffu, lb, 1);
+    if (lane == 31) {
+      ha = ta;
+      hb = tb;
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int d = r ? db : da;
+      if (d > d1) continue;
+      const uint32_t v = __funnelshift_r(r ? lb : la, r ? hb : ha, sh);
+      const int s0 = 4 * d - pos;  // piece offset of record byte 4d (>= -3)
+      if (s0 >= 0 && s0 + 3 < len) {
+        buf[d] = v;
+      } else {
+        const int k0 = max(0, -s0), k1 = min(3, len - 1 - s0);
+        const uint32_t mask = (0xffffffffu >> (8 * (3 - k1))) & (0xffffffffu << (8 * k0));
+        atomicOr(&buf[d], v & mask);
+      }
+    }
   }
+}
+
+// Record bytes [pos, pos + 4n) <- the 32-bit little-endian values v held by
+// lanes 0..n-1 (lane i's value at pos + 4i), merged with shared atomics.
+__device__ __forceinline__ void put_words(uint32_t* buf, int pos, uint32_t v, int n, int lane) {
+  if (lane >= n) return;
+  const int p = pos + 4 * lane;
+  const int w = p >> 2, sh = 8 * (p & 3);
+  if (w < kEmitWords) atomicOr(&buf[w], v << sh);
+  if (sh && w + 1 < kEmitWords) atomicOr(&buf[w + 1], v >> (32 - sh));
 }
 
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
@@ -1095,7 +1145,8 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
     const int mode = si.mode, k = si.param, body = si.body, n = si.count;
     const int rec_len = min(body + 3, kMaxRecordBytes);
     const int nwords = (rec_len + 3) >> 2;
-    for (int i = lane; i <= nwords; i += 32) buf[i] = 0;
+    // clear words 0 .. nwords (one past the record: the copy-out reads it)
+    for (int i = lane; 4 * i <= nwords; i += 32) reinterpret_cast<uint4*>(buf)[i] = make_uint4(0, 0, 0, 0);
     __syncwarp();
     if (lane == 0) atomicOr(&buf[0], static_cast<uint32_t>(mode) | (static_cast<uint32_t>(body & 0xffff) << 8));
     const uint32_t* __restrict__ f = folded + si.sample_base;
@@ -1106,10 +1157,12 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
       int cursor = 3;
       int run_start = 0;  // first index of the zero run reaching the chunk start
       const int nchunk = (n + 31) >> 5;
+      uint32_t v_next = lane < n ? __ldg(f + lane) : 1u;  // loaded one chunk ahead
       for (int m = 0; m < nchunk; ++m) {
         const int idx = m * 32 + lane;
         const bool valid = idx < n;
-        const uint32_t v = valid ? f[idx] : 1u;  // past the end acts as a terminator
+        const uint32_t v = v_next;  // past the end acts as a terminator
+        v_next = idx + 32 < n ? __ldg(f + idx + 32) : 1u;
         const uint32_t nzm = __ballot_sync(kFull, v != 0);
         const uint32_t below = nzm & ((1u << lane) - 1u);
         const int start = below ? m * 32 + (31 - __clz(below)) + 1 : run_start;
@@ -1150,20 +1203,42 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
         run_start = nzm ? m * 32 + (31 - __clz(nzm)) + 1 : run_start;
       }
     } else if (mode >= kModeRiceBase && mode <= kModeRiceBase + kMaxRice) {
+      // Rice lane c holds symbols c, c+4, ... (encode.cu:556-597; a shard of
+      // n < 4 symbols has n lanes of one symbol).  The warp takes 128 symbols
+      // at a time, lane j holding symbols 4j..4j+3: component c of every lane
+      // is then 32 consecutive codes of Rice lane c, placed by one warp scan
+      // of their lengths.  The next 128 symbols are loaded while these are
+      // placed.
       const int lane_count = min(4, n);
-      int64_t lane_off = 3 + static_cast<int64_t>(lane_count - 1) * 4;
-      if (lane < lane_count - 1) {
-        const uint32_t lb = static_cast<uint32_t>(si.comp_lane[lane]);
-        for (int b = 0; b < 4; ++b) put_byte(buf, 3 + lane * 4 + b, lb >> (8 * b));
+      put_words(buf, 3, lane < lane_count - 1 ? static_cast<uint32_t>(si.comp_lane[lane]) : 0u, lane_count - 1,
+                lane);
+      int64_t bb[4];  // bit cursor of each Rice lane
+      {
+        int off = 3 + 4 * (lane_count - 1);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          bb[c] = 8 * static_cast<int64_t>(off);
+          if (c < lane_count) off += si.comp_lane[c];
+        }
       }
       const uint32_t rmask = k == 0 ? 0u : (1u << k) - 1u;
-      for (int l = 0; l < lane_count; ++l) {
-        const int lsym = (n - l + lane_count - 1) / lane_count;
-        int64_t bitbase = lane_off * 8;
-        for (int g0 = 0; g0 < lsym; g0 += 32) {
-          const int li = g0 + lane;
-          const bool valid = li < lsym;
-          const uint32_t v = valid ? f[l + li * lane_count] : 0u;
+      const int nch = (n + 127) >> 7;
+      uint32_t nx[4];
+      auto load = [&](int m) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int idx = m * 128 + 4 * lane + c;
+          nx[c] = idx < n ? __ldg(f + idx) : 0u;
+        }
+      };
+      load(0);
+      for (int m = 0; m < nch; ++m) {
+        const uint32_t x[4] = {nx[0], nx[1], nx[2], nx[3]};
+        if (m + 1 < nch) load(m + 1);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const bool valid = m * 128 + 4 * lane + c < n;
+          const uint32_t v = x[c];
           const uint32_t q = v >> k;
           const uint32_t len = valid ? q + 1 + k : 0u;
           uint32_t inc = len;
@@ -1172,23 +1247,28 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
             const uint32_t t2 = __shfl_up_sync(kFull, inc, o);
             if (lane >= o) inc += t2;
           }
-          if (valid) {
-            const int64_t pos = bitbase + inc - len + q;
-            or_bits(buf, pos, 1u | ((v & rmask) << 1), k + 1);
-          }
-          bitbase += __shfl_sync(kFull, inc, 31);
+          if (valid) or_bits(buf, bb[c] + inc - len + q, 1u | ((v & rmask) << 1), k + 1);
+          bb[c] += __shfl_sync(kFull, inc, 31);
         }
-        lane_off += si.comp_lane[l];
       }
     } else if (mode == kModeBlockPack) {
       // widths and byte sizes of the (<= 32) blocks, one per lane
       const int nblk = (n + kBlockSymbols - 1) / kBlockSymbols;
       uint32_t my_w = 0;
-      for (int b = 0; b < nblk; ++b) {
-        uint32_t mx = 0;
-        for (int i = lane; i < kBlockSymbols && b * kBlockSymbols + i < n; i += 32) mx = max(mx, f[b * kBlockSymbols + i]);
-        mx = __reduce_max_sync(kFull, mx);
-        if (lane == b) my_w = bitlen(mx);
+      for (int b0 = 0; b0 < nblk; b0 += 4) {
+        uint32_t mx[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int i = 0; i < kBlockSymbols; i += 32) {
+            const int idx = (b0 + u) * kBlockSymbols + i + lane;
+            if (idx < n) mx[u] = max(mx[u], __ldg(f + idx));
+          }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const uint32_t m = __reduce_max_sync(kFull, mx[u]);
+          if (lane == b0 + u) my_w = bitlen(m);
+        }
       }
       const int my_n = lane < nblk ? min(kBlockSymbols, n - lane * kBlockSymbols) : 0;
       const uint32_t my_bytes = lane < nblk ? 1 + (my_n * my_w + 7) / 8 : 0;
@@ -1217,14 +1297,11 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
       const int tb = body - 28 - si.comp_lane[0] - si.comp_lane[1] - si.comp_lane[2] - si.comp_lane[3];
       put_bytes(buf, 3, ser, tb, lane);
       int pos = 3 + tb;
-      if (lane < 3) {
-        for (int b = 0; b < 4; ++b) put_byte(buf, pos + lane * 4 + b, static_cast<uint32_t>(si.comp_lane[lane]) >> (8 * b));
-      }
-      pos += 12;
-      if (lane < 4) {
-        for (int b = 0; b < 4; ++b) put_byte(buf, pos + lane * 4 + b, si.rans_state[lane] >> (8 * b));
-      }
-      pos += 16;
+      // three lane lengths, then four final states: seven words from lanes 0..6
+      const uint32_t lw = lane < 3 ? static_cast<uint32_t>(si.comp_lane[lane])
+                                   : (lane < 7 ? si.rans_state[lane - 3] : 0u);
+      put_words(buf, pos, lw, 7, lane);
+      pos += 28;
       for (int l = 0; l < 4; ++l) {
         const int len = si.comp_lane[l];
         const uint8_t* lane_end = base + kRansTableWords * 4 + kRansSerialBytes + (l + 1) * kRansLaneBytes;
@@ -1233,20 +1310,25 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
       }
     }
     __syncwarp();
-    // copy out: record bytes [0, rec_len) -> out + offset
+    // copy out: record bytes [0, rec_len) -> out + offset; byte stores up to
+    // the first 16-byte boundary of the destination, then one 16-byte store
+    // per lane (five record words funnel-shifted), then the ragged tail
     uint8_t* dst = outs[si.frame] + si.offset;
     const uint8_t* bytes = reinterpret_cast<const uint8_t*>(buf);
-    const int head = static_cast<int>((4 - (reinterpret_cast<uintptr_t>(dst) & 3)) & 3);
+    const int head = static_cast<int>((16 - (reinterpret_cast<uintptr_t>(dst) & 15)) & 15);
     const int hb = min(head, rec_len);
     if (lane < hb) dst[lane] = bytes[lane];
-    const int body_words = (rec_len - hb) >> 2;
-    uint32_t* dw = reinterpret_cast<uint32_t*>(dst + hb);
-    const int sh = hb * 8;
-    for (int j = lane; j < body_words; j += 32) {
-      const uint32_t lo = buf[j], hi = buf[j + 1];
-      dw[j] = sh ? __funnelshift_r(lo, hi, sh) : lo;
+    const int nvec = (rec_len - hb) >> 4;
+    uint4* dv = reinterpret_cast<uint4*>(dst + hb);
+    const int sh = 8 * (hb & 3);
+    const int w0 = hb >> 2;
+    for (int j = lane; j < nvec; j += 32) {
+      const uint32_t* b = buf + w0 + 4 * j;  // words up to w0 + 4 nvec <= nwords
+      const uint32_t a0 = b[0], a1 = b[1], a2 = b[2], a3 = b[3], a4 = b[4];
+      dv[j] = make_uint4(__funnelshift_r(a0, a1, sh), __funnelshift_r(a1, a2, sh), __funnelshift_r(a2, a3, sh),
+                         __funnelshift_r(a3, a4, sh));
     }
-    const int tail_start = hb + body_words * 4;
+    const int tail_start = hb + nvec * 16;
     if (lane < rec_len - tail_start) dst[tail_start + lane] = bytes[tail_start + lane];
     __syncwarp();
   }

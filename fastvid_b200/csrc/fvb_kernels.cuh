@@ -15,25 +15,26 @@ constexpr int kFastMaxW = 512;     // widest tile of the register-wavefront path
 #endif
 constexpr int kBlockUnroll = FVB_BLOCK_UNROLL;  // steps of a 32-step wavefront block unrolled
 
-// encoder
-__global__ void enc_init_kernel(const FrameDesc* frames, FrameState* state, int nframes);
-__global__ void enc_predict_kernel(const FrameDesc* frames, FrameState* state, int nframes,
-                                   int64_t total_tiles, ShardInfo* shards, uint32_t* folded, int* queue);
-__global__ void enc_predict_wide_kernel(const FrameDesc* frames, FrameState* state, int nframes,
-                                        int64_t total_tiles, uint32_t* folded, uint16_t* recon);
-__global__ void enc_analyze_kernel(const FrameDesc* frames, FrameState* state, int nframes, ShardInfo* shards,
-                                   int64_t total_shards, const uint32_t* folded, uint8_t* rans_scratch);
-__global__ void enc_rans_kernel(const FrameState* state, ShardInfo* shards, int64_t total_shards,
+// encoder (counts of pass `pass` from dims)
+__global__ void enc_init_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims);
+__global__ void enc_predict_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
+                                   ShardInfo* shards, uint32_t* folded, int* queue);
+__global__ void enc_predict_wide_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
+                                        uint32_t* folded, uint16_t* recon);
+__global__ void enc_analyze_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
+                                   ShardInfo* shards, const uint32_t* folded, uint8_t* rans_scratch);
+__global__ void enc_rans_kernel(const FrameState* state, const BatchDims* dims, int pass, ShardInfo* shards,
                                 const uint32_t* folded, uint8_t* rans_scratch);
-__global__ void enc_scan_kernel(const FrameDesc* frames, FrameState* state, int nframes, ShardInfo* shards,
-                                uint8_t* prefix);
+__global__ void enc_scan_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
+                                ShardInfo* shards, uint8_t* prefix);
 __global__ void enc_emit_kernel(const FrameDesc* frames, int nframes, const ShardInfo* shards,
                                 int64_t total_shards, const uint32_t* folded, const uint8_t* rans_scratch,
                                 uint8_t* const* outs);
 __global__ void enc_prefix_kernel(const FrameDesc* frames, int nframes, const uint8_t* prefix,
                                   uint8_t* const* outs);
 
-// decoder: shards binned by mode (0 rANS, 1 Rice, 2 zero-run, 3 block pack)
+// decoder: shards binned by mode (0 rANS, 1 Rice, 2 zero-run, 3 block pack);
+// counts from dims (entry 0)
 struct DecodeLists {
   int32_t count[4];
   int32_t next_group;       // dec_other work counter
@@ -41,22 +42,22 @@ struct DecodeLists {
   int32_t pad[2];
 };
 struct RansTable;
-__global__ void dec_parse_kernel(const FrameDesc* frames, FrameState* state, int nframes, int64_t total_tiles,
-                                 ShardInfo* shards, int64_t total_shards, DecodeLists* lists, int32_t* list_items);
+__global__ void dec_parse_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims,
+                                 ShardInfo* shards, DecodeLists* lists, int32_t* list_items);
 __global__ void dec_rans_tables_kernel(const FrameDesc* frames, FrameState* state, const ShardInfo* shards,
                                        const DecodeLists* lists, const int32_t* list_items, RansTable* tables);
 __global__ void dec_rans_kernel(const FrameDesc* frames, FrameState* state, const ShardInfo* shards,
                                 DecodeLists* lists, const int32_t* list_items, const RansTable* tables,
                                 uint32_t* folded);
 __global__ void dec_other_kernel(const FrameDesc* frames, FrameState* state, const ShardInfo* shards,
-                                 int64_t total_shards, DecodeLists* lists, const int32_t* list_items,
+                                 const BatchDims* dims, DecodeLists* lists, const int32_t* list_items,
                                  uint32_t* folded);
-__global__ void dec_reconstruct_kernel(const FrameDesc* frames, const FrameState* state, int nframes,
-                                       int64_t total_tiles, const uint32_t* folded, int* queue);
-__global__ void dec_reconstruct_wide_kernel(const FrameDesc* frames, const FrameState* state, int nframes,
-                                            int64_t total_tiles, const uint32_t* folded);
-__global__ void dec_reconstruct_serial_kernel(const FrameDesc* frames, const FrameState* state, int nframes,
-                                              int64_t total_tiles, const uint32_t* folded);
+__global__ void dec_reconstruct_kernel(const FrameDesc* frames, const FrameState* state, const BatchDims* dims,
+                                       const uint32_t* folded, int* queue);
+__global__ void dec_reconstruct_wide_kernel(const FrameDesc* frames, const FrameState* state, const BatchDims* dims,
+                                            const uint32_t* folded);
+__global__ void dec_reconstruct_serial_kernel(const FrameDesc* frames, const FrameState* state,
+                                              const BatchDims* dims, const uint32_t* folded);
 
 size_t enc_predict_smem();
 size_t enc_emit_smem();

@@ -77,6 +77,12 @@ class CodecBackend:
         self._plans: dict = {}    # request parameters and plane shapes -> Frame
 
     # ---- sizing (host only) ----
+    # A batch runs in its shape bucket's workspace: every count rounded up
+    # by at most 25 percent, with small floors; admission charges that bound.
+    @staticmethod
+    def _bucketed(ws: int) -> int:
+        return ws + ws // 4 + (2 << 20)
+
     def _encode_ws(self, frame: Frame) -> int:
         key = ("e", frame.layout, frame.bit_depth, frame.width, frame.height, frame.tile_w, frame.tile_h)
         ws = self._ws_cache.get(key)
@@ -115,7 +121,7 @@ class CodecBackend:
                 self._plans[key] = frame
         params = dict(layout=lay, bit_depth=bit_depth, quality=quality, frame_rate=tuple(frame_rate),
                       tile_size=tuple(tile_size))
-        return Request("encode", planes, params, frame.width * frame.height, self._encode_ws(frame),
+        return Request("encode", planes, params, frame.width * frame.height, self._bucketed(self._encode_ws(frame)),
                        frame.max_stream_bytes)
 
     def decode_request(self, stream: torch.Tensor, header: bytes | None = None,
@@ -132,13 +138,16 @@ class CodecBackend:
             if len(self._plans) < 4096:
                 self._plans[key] = frame
         return Request("decode", stream, dict(predictor=predictor, header=header), frame.width * frame.height,
-                       self._decode_ws(frame), 2 * frame.samples)
+                       self._bucketed(self._decode_ws(frame)), 2 * frame.samples)
 
     # ---- execution (worker threads) ----
     def make_worker_codec(self):
         from .batch import BatchCodec
 
-        return BatchCodec(self.device, use_graphs=False, resident_workspace=True)
+        # graphs per shape bucket: a worker replays the launch sequence of
+        # every bucket it has seen (captured thread-locally, beside the
+        # other workers' launches)
+        return BatchCodec(self.device, use_graphs=True, resident_workspace=True, max_cached_shapes=32)
 
     def resident_bytes(self, codec) -> int:
         return codec.workspace_bytes()

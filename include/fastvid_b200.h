@@ -4,8 +4,10 @@
  * Plain C types only: device pointers, sizes, an opaque CUDA stream handle
  * (a cudaStream_t passed as void*), and int status codes.  The caller owns
  * every buffer (workspace, inputs, outputs); the library allocates no device
- * memory.  Streams are byte-identical to the reference encoder
- * (generative-workflows/fastvid cuda/csrc/encode.cu) and decodes are bit-exact.
+ * memory.  Work runs on the device that owns the workspace; every entry point
+ * returns with the caller's current device unchanged.  Streams are
+ * byte-identical to the reference encoder (generative-workflows/fastvid
+ * cuda/csrc/encode.cu) and decodes are bit-exact.
  *
  * Status codes: 0 is success.  Positive codes are the reference's device
  * status codes, unchanged: encoder 1 = a sample above 2^bit_depth-1,
@@ -95,7 +97,8 @@ int fvb_encode_plan(int64_t width, int64_t height, int layout, int bit_depth, in
 /* Predicts, analyses and lays out the stream on `cuda_stream` (the frame
  * policy of encode.cu:812-847 runs on the device), then waits for the one
  * 96-byte result read and returns the exact stream length.  planes[p] are
- * device pointers to uint16 planes with row pitch pitches[p] (elements).
+ * device pointers to uint16 planes with row pitch pitches[p] (elements);
+ * host pointers return FVB_ERR_ARGUMENT before anything is launched.
  * Replaces encode.cu:727-870. */
 int fvb_encode_analyze(const fvb_frame* frame, const uint16_t* const* planes, const int64_t* pitches,
                        void* workspace, int64_t workspace_bytes, void* cuda_stream, int64_t* stream_len);
@@ -115,7 +118,9 @@ int fvb_decode_plan(const uint8_t* header, int64_t header_len, int64_t stream_le
 /* Decodes a device-resident stream into device planes (planes[p] with row
  * pitch pitches[p] elements), wavefront (1) or serial (0) reconstruction;
  * waits for the status word.  Replaces fastvid_decode_cuda
- * (cuda/csrc/decode.cu:660-730) including the device metadata parse. */
+ * (cuda/csrc/decode.cu:660-730) including the device metadata parse.
+ * The stream and the planes must be device (or managed) memory: a host
+ * pointer returns FVB_ERR_ARGUMENT before anything is launched. */
 int fvb_decode(const fvb_frame* frame, const uint8_t* stream, int64_t stream_len, uint16_t* const* planes,
                const int64_t* pitches, int wavefront, void* workspace, int64_t workspace_bytes,
                void* cuda_stream);
@@ -165,6 +170,43 @@ int fvb_batch_decode_prepare(const fvb_frame* frames, int n, const uint8_t* cons
 int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void* workspace,
                              int64_t workspace_bytes, int64_t* results, void* cuda_stream);
 
+/* ---- shape buckets (no reference counterpart) -----------------------------
+ *
+ * A bucket is a capacity: frames, tiles, shards, samples and header bytes of a
+ * batch (in total and per encoder pass), each rounded up to m * 2^e with m in
+ * 4..8 (at most 25 percent above the batch's), plus the exact pass count and
+ * wide-tile flag.  Workspace layout and launch grids follow the capacity and
+ * the kernels read the batch's actual counts from the workspace, so one
+ * enqueue -- and one CUDA graph captured from it -- serves every batch that
+ * fits the bucket, whatever its mix of frames.  The fvb_batch_* calls above
+ * are the same sequence with the batch's own totals as the capacity. */
+typedef struct fvb_bucket {
+  int64_t frames, tiles, shards, samples, prefix;
+  int64_t frames_p[3], tiles_p[3], shards_p[3]; /* per encoder pass */
+  int32_t passes, wide;
+} fvb_bucket;
+
+/* The bucket of a batch. */
+int fvb_batch_bucket(const fvb_frame* frames, int n, fvb_bucket* bucket);
+int fvb_bucket_encode_plan(const fvb_bucket* bucket, int64_t* workspace_bytes);
+int fvb_bucket_decode_plan(const fvb_bucket* bucket, int64_t* workspace_bytes);
+/* As the fvb_batch_* calls; the batch must fit the bucket (FVB_ERR_ARGUMENT
+ * otherwise).  Enqueue needs no frame list: everything it launches is sized
+ * by the bucket and reads the batch from the workspace.  `results` receives
+ * bucket->frames records (the batch's first). */
+int fvb_bucket_encode_prepare(const fvb_bucket* bucket, const fvb_frame* frames, int n,
+                              const uint16_t* const* planes, const int64_t* pitches, void* workspace,
+                              int64_t workspace_bytes, void* cuda_stream);
+int fvb_bucket_encode_enqueue(const fvb_bucket* bucket, void* workspace, int64_t workspace_bytes, int64_t* results,
+                              void* cuda_stream);
+int fvb_bucket_encode_emit(const fvb_bucket* bucket, const fvb_frame* frames, int n, void* workspace,
+                           int64_t workspace_bytes, uint8_t* const* outs, void* cuda_stream);
+int fvb_bucket_decode_prepare(const fvb_bucket* bucket, const fvb_frame* frames, int n,
+                              const uint8_t* const* streams, const int64_t* stream_lens, uint16_t* const* planes,
+                              const int64_t* pitches, void* workspace, int64_t workspace_bytes, void* cuda_stream);
+int fvb_bucket_decode_enqueue(const fvb_bucket* bucket, int wavefront, void* workspace, int64_t workspace_bytes,
+                              int64_t* results, void* cuda_stream);
+
 /* ---- allocation-free decode (no reference counterpart) --------------------
  *
  * For callers that cannot allocate device memory at decode time -- plug-ins
@@ -175,10 +217,14 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
  * the scratch is a fixed 32 MiB array inside the library
  * (fvb_decode_noalloc_capacity() bytes, frames up to about 7 million samples;
  * larger frames return FVB_ERR_WORKSPACE), so no workspace is passed and
- * nothing is allocated.  Every GPU that loads the library holds the array
- * until the process exits.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture.  All calls share the one array: calls whose work overlaps
+ * nothing is allocated: no device memory, no streams, no events (dec_other
+ * runs on the caller's stream).  Every GPU that loads the library holds the
+ * array until the process exits.  The first call on a device does the
+ * set-up: it looks up the array's device address (cudaGetSymbolAddress) and
+ * sets the kernels' shared-memory limits; make that first call before any
+ * stream capture.  The stream and the planes must be device (or managed)
+ * memory.  All calls share the one array, which keeps the last call's
+ * contents (every decode rewrites what it reads): calls whose work overlaps
  * on the GPU (other threads, other streams) race and must be serialised by
  * the caller; the call itself waits for its result before returning. */
 int64_t fvb_decode_noalloc_capacity(void);

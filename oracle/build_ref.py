@@ -10,6 +10,8 @@ on a GPU; it pins the CPU oracle through the golden fixtures made by
 tests/golden/make_golden.py.
 
 Usage: python oracle/build_ref.py [--reference PATH]
+The reference checkout is PATH, else $FASTVID_REFERENCE, else the location
+this recipe was written for (REFERENCE_CHECKOUT below).
 """
 
 from __future__ import annotations
@@ -21,6 +23,21 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
+# where the read-only reference checkout lives on the build machine; the GPU
+# hosts never read it (they use the module built into _ref/)
+REFERENCE_CHECKOUT = "/root/reference"
+
+
+def reference_dir() -> Path | None:
+    """The reference checkout, if one is present on this machine."""
+    path = Path(os.environ.get("FASTVID_REFERENCE", REFERENCE_CHECKOUT))
+    return path if (path / "cuda" / "csrc").is_dir() else None
+
+
+def built() -> Path | None:
+    """The built reference module, if any."""
+    found = sorted(OUT.glob("fastvid_ref_C*.so")) if OUT.is_dir() else []
+    return found[0] if found else None
 
 
 def build(reference: Path) -> Path:
@@ -49,9 +66,12 @@ def build(reference: Path) -> Path:
 
 def main() -> int:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference", default=None)
     args = parser.parse_args()
-    path = build(Path(args.reference))
+    ref = Path(args.reference) if args.reference else reference_dir()
+    if ref is None:
+        parser.error("no reference checkout found (pass --reference or set FASTVID_REFERENCE)")
+    path = build(ref)
     print(path)
     return 0
 

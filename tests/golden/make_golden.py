@@ -9,7 +9,7 @@ and writes:
                            SHA-256 of the decoded planes (uint16 LE, Y Cb Cr)
   streams/<case>.bin       the stream itself for cases below 64 KiB
 
-Usage: python tests/golden/make_golden.py [--out DIR]
+Usage: python tests/golden/make_golden.py [--out DIR] [--only CASE ...]
 Only valid inputs are given to the reference.
 """
 
@@ -55,12 +55,18 @@ def planes_sha(planes) -> str:
 def main() -> int:
     parser = argparse.ArgumentParser()
     parser.add_argument("--out", default=str(HERE))
+    parser.add_argument("--only", action="append", default=[],
+                        help="record only these cases and merge them into the existing file")
     args = parser.parse_args()
     out = Path(args.out)
     (out / "streams").mkdir(parents=True, exist_ok=True)
     ref = load_reference()
     records = {}
+    if args.only:
+        records = json.loads((out / "reference_streams.json").read_text())["cases"]
     for case in golden_cases.all_cases():
+        if args.only and case["name"] not in args.only:
+            continue
         planes = case["make"]()
         cuda_planes = [torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in planes]
         tw, th = case["tile"]

@@ -136,3 +136,27 @@ def test_host_pipelines_equal_the_device_path(cuda, mixed, chunk):
         assert len(got) == len(want)
         for g, w in zip(got, want):
             assert not g.is_cuda and np.array_equal(g.numpy(), w)
+
+
+def test_batches_of_one_bucket_replay_one_graph(cuda):
+    """Two batches of different frames whose counts fall into the same shape
+    bucket share one captured graph per direction, and each still writes the
+    oracle's bytes and planes."""
+    codec = BatchCodec(cuda)
+    base = [(640, 360, "rgb444", 8, 90, (64, 64)), (600, 352, "rgb444", 8, 90, (64, 64))]
+    batches = []
+    for seed, (w, h, layout, depth, q, tile) in enumerate(base):
+        frames = [dict(planes=synth.make_frame(w, h, layout, depth, 900 + 10 * seed + k), layout=layout,
+                       bit_depth=depth, quality=q, tile=tile) for k in range(3)]
+        batches.append(frames)
+    for frames in batches + batches:
+        streams = _encode(codec, frames)
+        planes = codec.decode(streams)
+        for f, st, pl in zip(frames, streams, planes):
+            exp = oracle.encode(f["planes"], layout=f["layout"], bit_depth=f["bit_depth"], quality=f["quality"],
+                                tile_size=f["tile"])
+            assert bytes(st.cpu().numpy().tobytes()) == exp
+            for a, b in zip(pl, oracle.decode(exp)):
+                assert np.array_equal(a.cpu().numpy(), b)
+    assert len(codec._enc) == 1 and len(codec._dec) == 1  # one bucket each way
+    assert codec.graph_kernels > 0  # later batches replayed the captured graphs

@@ -120,3 +120,72 @@ def test_decode_plan_accepts_valid_header_and_checks_directory_size():
     assert _native.last_error() == "truncated tile directory"
     assert _decode_plan(header[:20], size=20)[0] != 0
     assert _native.last_error() == "truncated Fastvid header"
+
+
+def test_host_pointers_are_rejected_before_any_launch():
+    """The single-frame entry points check that the stream and the planes are
+    device (or managed) memory; a host buffer returns FVB_ERR_ARGUMENT and
+    nothing is launched (on a CPU-only machine too)."""
+    import numpy as np
+
+    lib = _native.load()
+    planes = (np.arange(67 * 35, dtype=np.uint16).reshape(35, 67) % 256,)
+    stream = oracle.encode(planes, layout="gray", bit_depth=8, quality=100)
+    rc, frame = _decode_plan(stream[:32], size=len(stream))
+    assert rc == 0
+    host_stream = ctypes.create_string_buffer(stream, len(stream))
+    out = np.zeros(frame.samples, dtype=np.uint16)
+    ptrs = (ctypes.c_void_p * 3)(out.ctypes.data, 0, 0)
+    pitches = (ctypes.c_int64 * 3)(67, 0, 0)
+    before = lib.fvb_launch_count()
+    rc = lib.fvb_decode(ctypes.byref(frame), ctypes.addressof(host_stream), len(stream), ptrs, pitches, 1,
+                        None, 0, None)
+    assert rc == -1 and _native.last_error() == "encoded stream must be device memory"
+    rc = lib.fvb_decode_noalloc(ctypes.byref(frame), ctypes.addressof(host_stream), len(stream), ptrs, pitches,
+                                1, None)
+    assert rc == -1 and _native.last_error() == "encoded stream must be device memory"
+    rc, enc_frame, ws = _plan(67, 35, 0, 8, 100)
+    assert rc == 0
+    src = np.ascontiguousarray(planes[0])
+    length = ctypes.c_int64()
+    rc = lib.fvb_encode_analyze(ctypes.byref(enc_frame), (ctypes.c_void_p * 3)(src.ctypes.data, 0, 0),
+                                (ctypes.c_int64 * 3)(67, 0, 0), None, ws, None, ctypes.byref(length))
+    assert rc == -1 and _native.last_error() == "input planes must be device memory"
+    assert lib.fvb_launch_count() == before
+
+
+def test_batch_bucket_rounds_counts_up_by_at_most_a_quarter():
+    """fvb_batch_bucket: every count of the batch rounded up to m * 2^e with
+    m in 4..8 (so within 25 percent), small floors, exact passes and wide flag."""
+    from fastvid_b200._native import Bucket
+
+    lib = _native.load()
+    frames = []
+    for w, h, layout, depth, q, tile in [(1920, 1080, 2, 8, 90, (64, 64)), (2048, 1080, 0, 16, 87, (128, 128)),
+                                         (1280, 720, 0, 8, 100, (64, 64)), (301, 203, 1, 10, 80, (67, 35))]:
+        rc, frame, _ = _plan(w, h, layout, depth, q, tile=tile)
+        assert rc == 0
+        frames.append(frame)
+    arr = (Frame * len(frames))(*frames)
+    b = Bucket()
+    assert lib.fvb_batch_bucket(arr, len(frames), ctypes.byref(b)) == 0
+    tiles = sum(f.tiles for f in frames)
+    shards = sum(f.shards for f in frames)
+    samples = sum(f.samples for f in frames)
+    for actual, cap in ((len(frames), b.frames), (tiles, b.tiles), (shards, b.shards), (samples, b.samples)):
+        assert actual <= cap
+        if actual >= 8:
+            assert cap <= actual * 1.25
+            e = cap.bit_length() - 3
+            assert cap % (1 << max(e, 0)) == 0 and 4 <= cap >> max(e, 0) <= 8
+    assert b.passes == 3  # the gray16 q87 frame may refine its step twice
+    assert b.frames_p[1] >= 1 and b.frames_p[2] >= 1
+    assert b.wide == 0
+    ws = ctypes.c_int64()
+    assert lib.fvb_bucket_encode_plan(ctypes.byref(b), ctypes.byref(ws)) == 0 and ws.value > 0
+    exact = ctypes.c_int64()
+    assert lib.fvb_batch_encode_plan(arr, len(frames), ctypes.byref(exact)) == 0
+    assert exact.value <= ws.value <= 1.3 * exact.value + (4 << 20)
+    b.passes = 0
+    assert lib.fvb_bucket_encode_plan(ctypes.byref(b), ctypes.byref(ws)) == -1
+    assert _native.last_error() == "invalid bucket"

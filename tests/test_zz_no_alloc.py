@@ -36,10 +36,10 @@ def _plan(stream: torch.Tensor) -> Frame:
     return frame
 
 
-def _decode_noalloc(stream: torch.Tensor):
+def _decode_noalloc(stream: torch.Tensor, frame: Frame | None = None):
     """Decode through fvb_decode_noalloc into caller-owned planes."""
     lib = _native.load()
-    frame = _plan(stream)
+    frame = frame or _plan(stream)
     out = torch.empty(frame.samples, dtype=torch.uint16, device=stream.device)
     planes = plane_views(out, frame)
     ptrs = (ctypes.c_void_p * 3)(*[p.data_ptr() for p in planes] + [0] * (3 - len(planes)))
@@ -78,3 +78,38 @@ def test_noalloc_decode_rejects_frames_beyond_its_scratch(cuda):
     rc, _ = _decode_noalloc(stream)
     assert rc != 0
     assert "allocation-free decode" in _native.last_error()
+
+
+def test_noalloc_decode_leaves_no_state_behind_after_a_rejected_stream(cuda):
+    """A malformed stream decoded through the shared array fails, and the
+    next valid decode through the same array is still exact."""
+    good = _encode(640, 360, "rgb444", 10, 90, (64, 64), 105)
+    frame = _plan(good)
+    truncated = good[:-5].clone()  # the last tile's payload no longer ends at the stream end
+    rc, _ = _decode_noalloc(truncated, frame)
+    assert rc == 10, _native.last_error()
+    corrupt = good.clone()
+    mid = good.numel() // 2
+    corrupt[mid:mid + 64] ^= 0x5A  # damage entropy payload bytes
+    rc_corrupt, _ = _decode_noalloc(corrupt, frame)
+    assert rc_corrupt in (0, 1, 2, 3, 4, 5, 11)
+    for _ in range(2):
+        rc, got = _decode_noalloc(good)
+        assert rc == 0, _native.last_error()
+        for a, b in zip(got, fastvid_b200.decode(good)):
+            assert torch.equal(a, b)
+
+
+def test_noalloc_decode_rejects_a_host_stream_without_launching(cuda):
+    lib = _native.load()
+    good = _encode(320, 180, "gray", 10, 90, (64, 64), 106)
+    host = good.cpu()
+    frame = _plan(good)
+    out = torch.empty(frame.samples, dtype=torch.uint16, device=good.device)
+    ptrs = (ctypes.c_void_p * 3)(out.data_ptr(), 0, 0)
+    pitches = (ctypes.c_int64 * 3)(frame.width, 0, 0)
+    before = lib.fvb_launch_count()
+    rc = lib.fvb_decode_noalloc(ctypes.byref(frame), host.data_ptr(), host.numel(), ptrs, pitches, 1,
+                                torch.cuda.current_stream(good.device).cuda_stream)
+    assert rc == -1 and "device memory" in _native.last_error()
+    assert lib.fvb_launch_count() == before
