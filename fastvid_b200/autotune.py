@@ -1,12 +1,15 @@
 """Autotuner for the batched codec on one GPU.
 
-Two kinds of knob, tuned by measurement and kept in a JSON table:
+Three kinds of knob, tuned by measurement and kept in a JSON table:
 
 * Launch geometry -- the CTAs-per-SM cap of the persistent kernels
   (fvb_set_launch_ctas): how many tile wavefronts, analysis warps, rANS
   decode warps... share an SM.  No output byte depends on it.  Chosen by
   coordinate descent over the kernels on the measured encode+decode time of a
   sample batch.
+* Wavefront block -- how many of the 32 steps of each wavefront block the
+  predictor and reconstruction warps unroll (fvb_set_wavefront_block: 4, 8,
+  16 or 32).  No output byte depends on it; tuned before the launch caps.
 * Tile geometry per frame format (layout, depth, width, height) -- the
   wavefront block each warp sweeps.  The tile size is written into the
   stream header, so it changes the bytes and the compression; the tuner takes
@@ -32,6 +35,7 @@ TABLE = Path(__file__).resolve().parent / "tuning" / "b200.json"
 # kernels with a launch-geometry knob worth tuning, and the caps tried
 LAUNCH_KNOBS = ("enc_predict", "enc_analyze", "enc_emit", "dec_rans", "dec_other", "dec_reconstruct")
 LAUNCH_CANDIDATES = (2, 3, 4, 6, 8, 12, 16)
+WAVEFRONT_BLOCKS = (4, 8, 16, 32)
 TILE_CANDIDATES = ((32, 32), (64, 64), (128, 128))
 
 
@@ -99,9 +103,18 @@ def save(table: dict, path: Path | str = TABLE) -> None:
     Path(path).write_text(json.dumps(table, indent=1, sort_keys=True) + "\n")
 
 
+def wavefront_block() -> int:
+    return int(_native.load().fvb_get_wavefront_block())
+
+
+def set_wavefront_block(steps: int) -> None:
+    _native.check(_native.load().fvb_set_wavefront_block(int(steps)))
+
+
 def apply(table: dict) -> None:
-    """Set the table's launch geometry (process-wide)."""
+    """Set the table's launch geometry and wavefront block (process-wide)."""
     set_launch(table.get("launch", {}))
+    set_wavefront_block(table.get("wavefront_block", 0))
 
 
 def tile_for(table: dict | None, layout: str, bit_depth: int, width: int, height: int, default=(256, 128)):
@@ -144,6 +157,18 @@ def tune_launch(codec, frames, params, knobs=LAUNCH_KNOBS, candidates=LAUNCH_CAN
     best = descend(knobs, candidates, measure, start)
     set_launch(best)
     return best
+
+
+def tune_wavefront_block(codec, frames, params, candidates=WAVEFRONT_BLOCKS, reps: int = 3) -> tuple[int, dict]:
+    """The wavefront block with the lowest measured batch time (the launch
+    caps as currently set); returns it and every candidate's ms."""
+    seen = {}
+    for steps in candidates:
+        set_wavefront_block(steps)
+        seen[steps] = _time_batch(codec, frames, params, reps)[0]
+    best = min(seen, key=seen.get)
+    set_wavefront_block(best)
+    return best, {str(k): round(v, 3) for k, v in seen.items()}
 
 
 def tune_tiles(codec, groups: dict, candidates=TILE_CANDIDATES, size_tolerance: float = 0.02,
@@ -192,10 +217,12 @@ def main(argv=None) -> int:
                   tile_size=[tuple(tiles[format_key(s["layout"], s["bit_depth"], s["width"], s["height"])])
                              for s in specs])
     base_ms = _time_batch(codec, frames, params, args.reps)[0]
+    block, block_ms = tune_wavefront_block(codec, frames, params, reps=args.reps)
     launch = tune_launch(codec, frames, params, reps=args.reps)
     tuned_ms = _time_batch(codec, frames, params, args.reps)[0]
     table = {"device": torch.cuda.get_device_name(dev), "sample": f"{args.frames}-frame mix",
              "size_tolerance": args.size_tolerance, "tiles": tiles, "tile_measurements_ms_bytes": measured,
+             "wavefront_block": block, "wavefront_block_ms": block_ms,
              "launch": launch, "launch_gain": {"default_ms": round(base_ms, 3), "tuned_ms": round(tuned_ms, 3)}}
     save(table, args.out)
     print(json.dumps(table))

@@ -507,6 +507,93 @@ class BatchCodec:
         return out
 
 
+    def encode_decode_host(self, frames, *, chunk: int = 8, ahead: int = 3, predictor: str = "wavefront",
+                           out_streams: torch.Tensor | None = None, out_planes: torch.Tensor | None = None,
+                           **params):
+        """Encode frames held in (preferably pinned) host memory and decode
+        the streams again -- the round trip a codec evaluation makes -- with
+        the streams and the decoded planes delivered in pinned host memory
+        (views of `out_streams` / `out_planes` while they have room).
+
+        The frames go through in chunks of `chunk`: the upload of chunk
+        i+ahead, the encode and decode of chunk i, and the download of chunk
+        i-1's streams and planes run at once, on two copy streams beside the
+        compute stream, so both directions of the host link stay busy while
+        the kernels run.  The streams stay on the device between the encode
+        and the decode.  Streams equal encode()'s and planes decode()'s.
+        Returns (streams, planes), one entry per frame."""
+        n = len(frames)
+        if n == 0:
+            return [], []
+        frames = [tuple(f) if not isinstance(f, torch.Tensor) else (f,) for f in frames]
+        per = {k: _per_frame(v, n, k) for k, v in params.items()}
+        with torch.cuda.device(self.device):
+            comp = torch.cuda.current_stream(self.device)
+            h2d, d2h = torch.cuda.Stream(self.device), torch.cuda.Stream(self.device)
+            h2d.wait_stream(comp)
+            d2h.wait_stream(comp)
+            bounds = list(range(0, n, chunk)) + [n]
+            nchunks = len(bounds) - 1
+            staged: dict = {}
+
+            def stage(i):
+                lo, hi = bounds[i], bounds[i + 1]
+                with torch.cuda.stream(h2d):
+                    dev = [tuple(p.to(self.device, non_blocking=True) for p in f) for f in frames[lo:hi]]
+                    ev = torch.cuda.Event()
+                    ev.record(h2d)
+                staged[i] = (dev, ev)
+
+            def host_slice(buf, cursor, count, dtype):
+                if buf is not None and cursor + count <= buf.numel():
+                    return buf.narrow(0, cursor, count), cursor + count
+                return torch.empty(count, dtype=dtype, pin_memory=True), cursor
+
+            out_s, out_p = [], []
+            cur_s = cur_p = 0
+            for i in range(min(ahead, nchunks)):
+                stage(i)
+            for i in range(nchunks):
+                dev, ev = staged.pop(i)
+                comp.wait_event(ev)
+                for f in dev:
+                    for p in f:
+                        p.record_stream(comp)
+                lo, hi = bounds[i], bounds[i + 1]
+                streams = self.encode(dev, **{k: v[lo:hi] for k, v in per.items()})
+                planes = self.decode(streams, predictor=predictor)
+                if i + ahead < nchunks:
+                    stage(i + ahead)
+                done = torch.cuda.Event()
+                done.record(comp)
+                s_arena = streams[0]._base if streams[0]._base is not None else streams[0]
+                first = planes[0][0]
+                p_arena = first._base if first._base is not None else first
+                s_total = sum(int(st.numel()) for st in streams)
+                p_total = sum(p.numel() for f in planes for p in f)
+                hs, cur_s = host_slice(out_streams, cur_s, s_total, torch.uint8)
+                hp, cur_p = host_slice(out_planes, cur_p, p_total, torch.uint16)
+                with torch.cuda.stream(d2h):
+                    d2h.wait_event(done)
+                    s_arena.record_stream(d2h)
+                    p_arena.record_stream(d2h)
+                    hs.copy_(s_arena.narrow(0, 0, s_total), non_blocking=True)
+                    hp.copy_(p_arena.reshape(-1).narrow(0, 0, p_total), non_blocking=True)
+                off = 0
+                for st in streams:
+                    out_s.append(hs.narrow(0, off, st.numel()))
+                    off += st.numel()
+                off = 0
+                for f in planes:
+                    views = []
+                    for p in f:
+                        views.append(hp.narrow(0, off, p.numel()).view(p.shape))
+                        off += p.numel()
+                    out_p.append(tuple(views))
+            d2h.synchronize()
+        return out_s, out_p
+
+
 _default: dict = {}
 
 

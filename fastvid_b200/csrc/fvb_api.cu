@@ -273,12 +273,10 @@ int ensure_smem_attrs() {
   int dev = 0;
   FVB_CUDA(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && done[dev]) return FVB_OK;
-  FVB_CUDA(cudaFuncSetAttribute(enc_predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(enc_predict_smem())));
+  FVB_CUDA(enc_predict_set_smem());
   FVB_CUDA(cudaFuncSetAttribute(enc_emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(enc_emit_smem())));
-  FVB_CUDA(cudaFuncSetAttribute(dec_reconstruct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(dec_reconstruct_smem())));
+  FVB_CUDA(dec_reconstruct_set_smem());
   FVB_CUDA(cudaFuncSetAttribute(dec_rans_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(dec_rans_smem())));
   // the whole unified L1/shared array as shared memory: four dec_rans CTAs
@@ -579,6 +577,7 @@ constexpr int kDefaultCtas[K_COUNT] = {
     /*dec_reconstruct*/ 4, /*dec_reconstruct_wide*/ 8, /*dec_reconstruct_serial*/ 0, /*results*/ 0,
     /*dec_rans*/ 16, /*dec_other*/ 16};
 std::atomic<int> g_ctas[K_COUNT];
+std::atomic<int> g_wavefront_block{kDefaultWavefrontBlock};
 
 int ctas(int kernel) {
   const int v = g_ctas[kernel].load(std::memory_order_relaxed);
@@ -640,6 +639,16 @@ int fvb_get_launch_ctas(int kernel) {
   if (kernel < 0 || kernel >= K_COUNT || kDefaultCtas[kernel] == 0) return -1;
   return ctas(kernel);
 }
+
+int fvb_set_wavefront_block(int steps) {
+  if (steps == 0) steps = kDefaultWavefrontBlock;
+  if (steps != 4 && steps != 8 && steps != 16 && steps != 32)
+    return fail(FVB_ERR_ARGUMENT, "wavefront block must be 4, 8, 16 or 32 steps");
+  g_wavefront_block.store(steps, std::memory_order_relaxed);
+  return FVB_OK;
+}
+
+int fvb_get_wavefront_block(void) { return g_wavefront_block.load(std::memory_order_relaxed); }
 
 const char* fvb_kernel_name(int kernel) { return kernel >= 0 && kernel < K_COUNT ? kKernelNames[kernel] : ""; }
 
@@ -810,8 +819,9 @@ int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, 
     FVB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), stream));
     {
       LaunchScope scope_(K_ENC_PREDICT, stream);
-      enc_predict_kernel<<<grid_for(tiles, kWarpsPerCta, ctas(K_ENC_PREDICT)), kWarpsPerCta * 32, enc_predict_smem(), stream>>>(
-          frames_d, state, dims, pass, shards, folded, queue);
+      enc_predict_launch(g_wavefront_block.load(std::memory_order_relaxed),
+                         grid_for(tiles, kWarpsPerCta, ctas(K_ENC_PREDICT)), stream, frames_d, state, dims, pass,
+                         shards, folded, queue);
     }
     FVB_LAUNCHED("enc_predict_kernel");
     if (cap.wide) {
@@ -1188,8 +1198,9 @@ int decode_enqueue(const Totals& t, int wavefront, void* workspace, int64_t work
   if (wavefront) {
     {
       LaunchScope scope_(K_DEC_RECON, stream);
-      dec_reconstruct_kernel<<<grid_for(t.tiles, kWarpsPerCta, ctas(K_DEC_RECON)), kWarpsPerCta * 32, dec_reconstruct_smem(), stream>>>(
-          frames_d, state, dims, folded, queue);
+      dec_reconstruct_launch(g_wavefront_block.load(std::memory_order_relaxed),
+                             grid_for(t.tiles, kWarpsPerCta, ctas(K_DEC_RECON)), stream, frames_d, state, dims, folded,
+                             queue);
     }
     FVB_LAUNCHED("dec_reconstruct_kernel");
     if (t.wide) {

@@ -821,13 +821,13 @@ struct RecWarpSmem {
 
 size_t dec_reconstruct_smem() { return sizeof(RecWarpSmem) * kWarpsPerCta; }
 
-template <bool MED, bool STEP1, bool EDGE>
+template <bool MED, bool STEP1, bool EDGE, int UNROLL>
 __device__ __forceinline__ void rec_block(RecWarpSmem& sm, int lane, int t0, int W, int32_t maxs, int32_t step,
                                           bool band0, int32_t& rec, int32_t& a_prev) {
   const uint32_t* frow = sm.fold + lane * kFoldStride + (t0 & 32);
   uint16_t* orow = sm.out + lane * kSrcStride + (t0 & 32);
   uint16_t* crow = sm.carry + 32 - lane + t0;
-#pragma unroll kBlockUnroll
+#pragma unroll UNROLL
   for (int u = 0; u < 32; ++u) {
     const uint32_t fv = frow[u];
     int32_t a = __shfl_up_sync(0xffffffffu, rec, 1);
@@ -849,7 +849,7 @@ __device__ __forceinline__ void rec_block(RecWarpSmem& sm, int lane, int t0, int
   }
 }
 
-template <bool MED, bool STEP1>
+template <bool MED, bool STEP1, int UNROLL>
 __device__ void rec_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step,
                               const uint32_t* __restrict__ ftile, RecWarpSmem& sm, int lane) {
   uint16_t* __restrict__ plane = f.dst[g.plane];
@@ -905,8 +905,8 @@ __device__ void rec_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
         if (blk + 1 < nchunks) load_chunk(blk + 1);
       }
       const int t0 = blk * 32;
-      if (t0 < 31 || t0 + 31 >= W) rec_block<MED, STEP1, true>(sm, lane, t0, W, maxs, step, band0, rec, a_prev);
-      else rec_block<MED, STEP1, false>(sm, lane, t0, W, maxs, step, band0, rec, a_prev);
+      if (t0 < 31 || t0 + 31 >= W) rec_block<MED, STEP1, true, UNROLL>(sm, lane, t0, W, maxs, step, band0, rec, a_prev);
+      else rec_block<MED, STEP1, false, UNROLL>(sm, lane, t0, W, maxs, step, band0, rec, a_prev);
     }
     __syncwarp();
     for (int j = max(0, nblocks - 2); j < nchunks; ++j) flush_chunk(j);
@@ -914,6 +914,7 @@ __device__ void rec_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
   }
 }
 
+template <int UNROLL>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
 dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
                        const BatchDims* __restrict__ dims, const uint32_t* __restrict__ folded,
@@ -935,13 +936,34 @@ dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* _
     if (g.w > kFastMaxW) continue;
     const uint32_t* ftile = folded + f.sample_base + g.sample_base;
     if (f.use_med0) {
-      if (f.step0 == 1) rec_tile_fast<true, true>(f, g, 1, ftile, sm, lane);
-      else rec_tile_fast<true, false>(f, g, f.step0, ftile, sm, lane);
+      if (f.step0 == 1) rec_tile_fast<true, true, UNROLL>(f, g, 1, ftile, sm, lane);
+      else rec_tile_fast<true, false, UNROLL>(f, g, f.step0, ftile, sm, lane);
     } else {
-      if (f.step0 == 1) rec_tile_fast<false, true>(f, g, 1, ftile, sm, lane);
-      else rec_tile_fast<false, false>(f, g, f.step0, ftile, sm, lane);
+      if (f.step0 == 1) rec_tile_fast<false, true, UNROLL>(f, g, 1, ftile, sm, lane);
+      else rec_tile_fast<false, false, UNROLL>(f, g, f.step0, ftile, sm, lane);
     }
   }
+}
+
+// The wavefront block of dec_reconstruct is a launch-time choice, as for
+// enc_predict (4, 8, 16 or 32 steps unrolled; identical planes).
+cudaError_t dec_reconstruct_set_smem() {
+  const int bytes = static_cast<int>(dec_reconstruct_smem());
+  for (auto k : {dec_reconstruct_kernel<4>, dec_reconstruct_kernel<8>, dec_reconstruct_kernel<16>,
+                 dec_reconstruct_kernel<32>}) {
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+void dec_reconstruct_launch(int unroll, int grid, cudaStream_t stream, const FrameDesc* frames,
+                            const FrameState* state, const BatchDims* dims, const uint32_t* folded, int* queue) {
+  auto k = unroll == 4    ? dec_reconstruct_kernel<4>
+           : unroll == 16 ? dec_reconstruct_kernel<16>
+           : unroll == 32 ? dec_reconstruct_kernel<32>
+                          : dec_reconstruct_kernel<8>;
+  k<<<grid, kWarpsPerCta * 32, dec_reconstruct_smem(), stream>>>(frames, state, dims, folded, queue);
 }
 
 // Wide tiles: antidiagonal order with neighbours read back from the output

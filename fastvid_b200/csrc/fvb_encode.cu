@@ -59,14 +59,14 @@ struct EncWarpSmem {
   uint16_t carry[kFastMaxW + 128];  // row above the band, column c at index c + 32
 };
 
-template <bool MED, bool STEP1, bool EDGE>
+template <bool MED, bool STEP1, bool EDGE, int UNROLL>
 __device__ __forceinline__ void enc_block(EncWarpSmem& sm, int lane, int t0, int W,
                                           int32_t maxs, int32_t step, int32_t half, uint32_t magic, bool band0,
                                           int32_t& rec, int32_t& a_prev) {
   const uint16_t* srow = sm.src + lane * kSrcStride + (t0 & 32);
   uint32_t* frow = sm.fold + lane * kFoldStride + (t0 & 32);
   uint16_t* crow = sm.carry + 32 - lane + t0;  // carry index (t - lane) + 32
-#pragma unroll kBlockUnroll
+#pragma unroll UNROLL
   for (int u = 0; u < 32; ++u) {
     const int32_t s = srow[u];
     int32_t a = __shfl_up_sync(0xffffffffu, rec, 1);
@@ -96,7 +96,7 @@ __device__ __forceinline__ void enc_block(EncWarpSmem& sm, int lane, int t0, int
   }
 }
 
-template <bool MED, bool STEP1>
+template <bool MED, bool STEP1, int UNROLL>
 __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step, uint32_t magic,
                               uint32_t* __restrict__ folded_tile, EncWarpSmem& sm, int lane, int32_t& bad) {
   const uint16_t* __restrict__ plane = f.src[g.plane];
@@ -157,8 +157,8 @@ __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
       }
       const int t0 = blk * 32;
       const bool edge = t0 < 31 || t0 + 31 >= W;
-      if (edge) enc_block<MED, STEP1, true>(sm, lane, t0, W, maxs, step, half, magic, band0, rec, a_prev);
-      else enc_block<MED, STEP1, false>(sm, lane, t0, W, maxs, step, half, magic, band0, rec, a_prev);
+      if (edge) enc_block<MED, STEP1, true, UNROLL>(sm, lane, t0, W, maxs, step, half, magic, band0, rec, a_prev);
+      else enc_block<MED, STEP1, false, UNROLL>(sm, lane, t0, W, maxs, step, half, magic, band0, rec, a_prev);
     }
     __syncwarp();
     for (int j = max(0, nblocks - 2); j < nchunks; ++j) flush_chunk(j);
@@ -167,6 +167,7 @@ __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
   if (vmax > static_cast<uint32_t>(maxs)) bad = 1;
 }
 
+template <int UNROLL>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
 enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
                    const BatchDims* __restrict__ dims, int pass, ShardInfo* __restrict__ shards,
@@ -201,14 +202,35 @@ enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     int32_t bad = 0;
     const bool med = st.use_med != 0;
     if (med) {
-      if (step == 1) enc_tile_fast<true, true>(f, g, step, magic, ftile, sm, lane, bad);
-      else enc_tile_fast<true, false>(f, g, step, magic, ftile, sm, lane, bad);
+      if (step == 1) enc_tile_fast<true, true, UNROLL>(f, g, step, magic, ftile, sm, lane, bad);
+      else enc_tile_fast<true, false, UNROLL>(f, g, step, magic, ftile, sm, lane, bad);
     } else {
-      if (step == 1) enc_tile_fast<false, true>(f, g, step, magic, ftile, sm, lane, bad);
-      else enc_tile_fast<false, false>(f, g, step, magic, ftile, sm, lane, bad);
+      if (step == 1) enc_tile_fast<false, true, UNROLL>(f, g, step, magic, ftile, sm, lane, bad);
+      else enc_tile_fast<false, false, UNROLL>(f, g, step, magic, ftile, sm, lane, bad);
     }
     if (__any_sync(kFull, bad) && lane == 0) set_status(&st.status, 1);
   }
+}
+
+// The wavefront block of enc_predict -- steps of each 32-step block unrolled
+// -- is a launch-time choice (4, 8, 16 or 32; the autotuner's knob): every
+// choice computes the same bytes.
+cudaError_t enc_predict_set_smem() {
+  const int bytes = static_cast<int>(enc_predict_smem());
+  for (auto k : {enc_predict_kernel<4>, enc_predict_kernel<8>, enc_predict_kernel<16>, enc_predict_kernel<32>}) {
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+void enc_predict_launch(int unroll, int grid, cudaStream_t stream, const FrameDesc* frames, FrameState* state,
+                        const BatchDims* dims, int pass, ShardInfo* shards, uint32_t* folded, int* queue) {
+  auto k = unroll == 4    ? enc_predict_kernel<4>
+           : unroll == 16 ? enc_predict_kernel<16>
+           : unroll == 32 ? enc_predict_kernel<32>
+                          : enc_predict_kernel<8>;
+  k<<<grid, kWarpsPerCta * 32, enc_predict_smem(), stream>>>(frames, state, dims, pass, shards, folded, queue);
 }
 
 // Tiles wider than kFastMaxW: one CTA per tile walks the antidiagonals with

@@ -10,15 +10,14 @@ constexpr int kWarpsPerCta = 4;    // warps per CTA of the warp-per-item kernels
 constexpr int kSrcStride = 66;     // u16 ring row stride: 64 columns + 2 (33 words: conflict-free)
 constexpr int kFoldStride = 65;    // u32 ring row stride: 64 columns + 1 (conflict-free)
 constexpr int kFastMaxW = 512;     // widest tile of the register-wavefront path
-#ifndef FVB_BLOCK_UNROLL
-#define FVB_BLOCK_UNROLL 8
-#endif
-constexpr int kBlockUnroll = FVB_BLOCK_UNROLL;  // steps of a 32-step wavefront block unrolled
+constexpr int kDefaultWavefrontBlock = 8;  // steps of a 32-step wavefront block unrolled (4, 8, 16, 32)
 
 // encoder (counts of pass `pass` from dims)
 __global__ void enc_init_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims);
-__global__ void enc_predict_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
-                                   ShardInfo* shards, uint32_t* folded, int* queue);
+// enc_predict with a wavefront block of `unroll` steps (4, 8, 16, 32)
+void enc_predict_launch(int unroll, int grid, cudaStream_t stream, const FrameDesc* frames, FrameState* state,
+                        const BatchDims* dims, int pass, ShardInfo* shards, uint32_t* folded, int* queue);
+cudaError_t enc_predict_set_smem();
 __global__ void enc_predict_wide_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
                                         uint32_t* folded, uint16_t* recon);
 __global__ void enc_analyze_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
@@ -52,8 +51,9 @@ __global__ void dec_rans_kernel(const FrameDesc* frames, FrameState* state, cons
 __global__ void dec_other_kernel(const FrameDesc* frames, FrameState* state, const ShardInfo* shards,
                                  const BatchDims* dims, DecodeLists* lists, const int32_t* list_items,
                                  uint32_t* folded);
-__global__ void dec_reconstruct_kernel(const FrameDesc* frames, const FrameState* state, const BatchDims* dims,
-                                       const uint32_t* folded, int* queue);
+void dec_reconstruct_launch(int unroll, int grid, cudaStream_t stream, const FrameDesc* frames,
+                            const FrameState* state, const BatchDims* dims, const uint32_t* folded, int* queue);
+cudaError_t dec_reconstruct_set_smem();
 __global__ void dec_reconstruct_wide_kernel(const FrameDesc* frames, const FrameState* state, const BatchDims* dims,
                                             const uint32_t* folded);
 __global__ void dec_reconstruct_serial_kernel(const FrameDesc* frames, const FrameState* state,

@@ -216,6 +216,7 @@ class Server:
         self.batches: list[tuple[str, int]] = []  # (kind, size) of every batch run
         self.batch_times: list[tuple[float, float, str, int, int]] = []  # (start, end, kind, size, pixels)
         self.max_concurrent = 0
+        self.peak_charged = 0  # largest resident + in-flight bytes charged against the budget
         self._threads = [threading.Thread(target=self._worker, args=(i,), daemon=True) for i in range(workers)]
         for t in self._threads:
             t.start()
@@ -292,6 +293,7 @@ class Server:
         self._inflight += out
         self._running += 1
         self.max_concurrent = max(self.max_concurrent, self._running)
+        self.peak_charged = max(self.peak_charged, sum(self._resident) + self._inflight)
         return kind, chosen, out
 
     def _worker(self, w: int):
@@ -346,6 +348,7 @@ class Server:
                 self._inflight -= out
                 self._running -= 1
                 self._resident[w] = max(self.backend.resident_bytes(codec), 0)
+                self.peak_charged = max(self.peak_charged, sum(self._resident) + self._inflight)
                 self.batches.append((kind, len(reqs)))
                 self._cv.notify_all()
 

@@ -74,8 +74,10 @@ class PlaneSpec:
     sigma_den: int = 1
 
 
-def _field(width: int, height: int, rng: np.random.Generator, amplitude: int) -> np.ndarray:
-    """Zero-mean sum of 4 sinusoid layers with amplitudes summing to `amplitude`."""
+def _field(width: int, height: int, rng: np.random.Generator, amplitude: int,
+           min_period: int = 32) -> np.ndarray:
+    """Zero-mean sum of 4 sinusoid layers with amplitudes summing to `amplitude`
+    and periods between `min_period` and 256 px."""
     table = _sine_table()
     y = np.arange(height, dtype=np.int64)[:, None]
     x = np.arange(width, dtype=np.int64)[None, :]
@@ -83,11 +85,13 @@ def _field(width: int, height: int, rng: np.random.Generator, amplitude: int) ->
     amps = (weights * amplitude) // weights.sum()
     out = np.zeros((height, width), dtype=np.int64)
     for a in amps:
-        # spatial frequency |k| in [1024, 8192] table units / 256 px -> periods 32..256 px
+        # spatial frequency |k| in [1024, kmax] table units / 256 px -> periods
+        # min_period..256 px (kmax = 8192 for 32 px)
+        kmax = (256 * 1024) // min_period
         while True:
-            kx, ky = (int(v) for v in rng.integers(-8192, 8193, size=2))
+            kx, ky = (int(v) for v in rng.integers(-kmax, kmax + 1, size=2))
             n2 = kx * kx + ky * ky
-            if 1024 * 1024 <= n2 <= 8192 * 8192:
+            if 1024 * 1024 <= n2 <= kmax * kmax:
                 break
         phase = int(rng.integers(0, 1 << _TABLE_BITS))
         arg = ((x * kx + y * ky) >> 8) + phase
@@ -107,11 +111,12 @@ def _rectangles(plane: np.ndarray, rng: np.random.Generator, count: int, maximum
 
 def make_frame(width: int, height: int, layout: str, bit_depth: int, seed: int, *,
                amplitude: int | None = None, mean: int | None = None, rects: int = 10,
-               sigma: tuple[int, int] = (2, 1), correlation: bool = True):
+               sigma: tuple[int, int] = (2, 1), correlation: bool = True, min_period: int = 32):
     """One frame as a tuple of (H, W) uint16 numpy planes.
 
     `sigma` is a rational (numerator, denominator).  For rgb444 the sinusoid
     fields are correlated across planes (0.8 shared + 0.6 independent).
+    `min_period` (32..256) is the shortest sinusoid period in pixels.
     """
     maximum = (1 << bit_depth) - 1
     if mean is None:
@@ -121,11 +126,11 @@ def make_frame(width: int, height: int, layout: str, bit_depth: int, seed: int, 
     rng = np.random.default_rng(seed)
     plane_count = 1 if layout == "gray" else 3
     widths = [width] + [((width + 1) // 2) if layout == "yuv422" else width] * (plane_count - 1)
-    shared = _field(width, height, rng, amplitude) if (layout == "rgb444" and correlation) else None
+    shared = _field(width, height, rng, amplitude, min_period) if (layout == "rgb444" and correlation) else None
     planes = []
     for p in range(plane_count):
         pw = widths[p]
-        field = _field(pw, height, rng, amplitude)
+        field = _field(pw, height, rng, amplitude, min_period)
         if shared is not None:
             field = (4 * shared + 3 * field) // 5
         plane = field + mean
@@ -145,6 +150,13 @@ CONFIGS = {
                       gen=dict(seed=5, rects=20, sigma=(40, 1), amplitude=20000, mean=32768)),
     "rgb10_4k": dict(width=3840, height=2160, layout="rgb444", bit_depth=10, quality=85, tile=(128, 128),
                      gen=dict(seed=6, rects=10, sigma=(4, 1))),
+    # gray16 4K whose baseline payload at step 556 exceeds 0.5 B/sample, so the
+    # encoder's frame policy refines the step to 417 (header flag 0x80).  With
+    # noise sd 40 the payload stays between 0.1 and 0.5 B/sample for every
+    # seed tried (1..40, and with sinusoid periods held to 64..256 px) and the
+    # step stays 556; sd 1000 is the smallest round value found that refines.
+    "gray16_4k_step417": dict(width=3840, height=2160, layout="gray", bit_depth=16, quality=87, tile=(128, 128),
+                              gen=dict(seed=5, rects=20, sigma=(1000, 1), amplitude=20000, mean=32768)),
 }
 
 
@@ -209,8 +221,9 @@ def reference_pattern(layout: str, width: int, height: int, bit_depth: int, patt
 
 # The serving mix: formats drawn with weights 0.3 720p gray8, 0.4 1080p RGB8,
 # 0.2 4K RGB10, 0.1 4K gray16; quality giving steps {1, 3, 7} (8/10-bit) or
-# {1, 417/556} (16-bit; gray8 is always lossless); 60% encode, 40% decode of
-# streams produced earlier.
+# {1, 417} (16-bit: the gray16 frames carry noise sd 1000, so q87 refines to
+# step 417; gray8 is always lossless); 60% encode, 40% decode of streams
+# produced earlier.
 SERVING_FORMATS = [
     (0.3, dict(width=1280, height=720, layout="gray", bit_depth=8, qualities=(100,), tile=(64, 64))),
     (0.4, dict(width=1920, height=1080, layout="rgb444", bit_depth=8, qualities=(100, 90, 66), tile=(64, 64))),
@@ -243,4 +256,4 @@ def serving_frame(fmt: int, index: int, scale: int = 1):
     return make_frame(f["width"] // scale, f["height"] // scale, f["layout"], depth, 7000 + 97 * fmt + index,
                       amplitude=20000 if depth == 16 else None, mean=32768 if depth == 16 else None,
                       rects=20 if depth == 16 else 10,
-                      sigma=(40, 1) if depth == 16 else ((4, 1) if depth == 10 else (3, 1)))
+                      sigma=(1000, 1) if depth == 16 else ((4, 1) if depth == 10 else (3, 1)))

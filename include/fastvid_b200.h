@@ -75,6 +75,14 @@ const char* fvb_kernel_name(int kernel);
 int fvb_set_launch_ctas(int kernel, int ctas_per_sm);
 /* The cap in effect, or -1 for a kernel without the knob. */
 int fvb_get_launch_ctas(int kernel);
+/* Wavefront block of the predictor and reconstruction kernels (no
+ * counterpart in the reference, whose predictor walks antidiagonals with a
+ * barrier per step, cuda/csrc/encode.cu:150-192): each warp sweeps 32-row
+ * bands in blocks of 32 steps, `steps` (4, 8, 16 or 32) of them unrolled;
+ * 0 restores the default (8).  Process-wide, read at each launch; no output
+ * depends on it (the autotuner's knob). */
+int fvb_set_wavefront_block(int steps);
+int fvb_get_wavefront_block(void);
 /* While profiling is on (per calling thread), every launch is bracketed by
  * CUDA events on its stream; fvb_profile_end waits for them and writes, per
  * kernel id, the summed milliseconds and the number of launches. */

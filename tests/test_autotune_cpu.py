@@ -66,3 +66,21 @@ def test_table_round_trip(tmp_path):
         assert autotune.launch_settings()["enc_emit"] == 6
     finally:
         autotune.reset_launch()
+
+
+def test_wavefront_block_knob_round_trip_and_rejections():
+    lib = _native.load()
+    before = autotune.wavefront_block()
+    try:
+        for steps in autotune.WAVEFRONT_BLOCKS:
+            autotune.set_wavefront_block(steps)
+            assert autotune.wavefront_block() == steps
+        for bad in (1, 3, 12, 64, -8):
+            assert lib.fvb_set_wavefront_block(bad) == -1
+            assert "wavefront block" in _native.last_error()
+        autotune.set_wavefront_block(0)
+        assert autotune.wavefront_block() == 8  # the default
+        autotune.apply({"launch": {}, "wavefront_block": 16})
+        assert autotune.wavefront_block() == 16
+    finally:
+        autotune.set_wavefront_block(before)

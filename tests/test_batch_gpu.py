@@ -160,3 +160,23 @@ def test_batches_of_one_bucket_replay_one_graph(cuda):
                 assert np.array_equal(a.cpu().numpy(), b)
     assert len(codec._enc) == 1 and len(codec._dec) == 1  # one bucket each way
     assert codec.graph_kernels > 0  # later batches replayed the captured graphs
+
+
+def test_host_round_trip_matches_device_batch(cuda, mixed):
+    """encode_decode_host (pinned frames in, streams and planes out, copies
+    overlapping the kernels chunk by chunk) returns the oracle's streams and
+    planes, with a chunk size that splits the batch unevenly and an output
+    buffer too small for all of it."""
+    codec = BatchCodec(cuda)
+    pinned = [tuple(torch.from_numpy(np.ascontiguousarray(p)).pin_memory() for p in f["planes"]) for f in mixed]
+    total_bytes = sum(len(f["oracle"]) for f in mixed)
+    out_s = torch.empty(total_bytes // 2, dtype=torch.uint8).pin_memory()  # later chunks get new buffers
+    streams, planes = codec.encode_decode_host(pinned, chunk=5, layout=[f["layout"] for f in mixed],
+                                               bit_depth=[f["bit_depth"] for f in mixed],
+                                               quality=[f["quality"] for f in mixed],
+                                               tile_size=[f["tile"] for f in mixed], out_streams=out_s)
+    assert len(streams) == len(planes) == len(mixed)
+    for f, st, pl in zip(mixed, streams, planes):
+        assert not st.is_cuda and bytes(st.numpy().tobytes()) == f["oracle"]
+        for a, b in zip(pl, oracle.decode(f["oracle"])):
+            assert not a.is_cuda and np.array_equal(a.numpy(), b)

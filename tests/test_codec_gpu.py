@@ -148,6 +148,20 @@ def test_stream_bytes_match_reference(cuda, case):
         assert _sha_planes(decoded_host) == rec["decoded_sha256"]
 
 
+def test_config_3a_gray16_4k_refines_to_step_417(cuda):
+    """3840x2160 gray16 q87: the reference's frame policy refines the step
+    from 556 to 417 (header flag 0x80, encode.cu:826-840); so does this one."""
+    rec = RECORDS["cfg_gray16_4k_step417"]
+    assert rec["flags"] == 0x88  # refined gray16 (0x80) | depth 16 (0x08), as the reference wrote it
+    case = golden_cases.case_map()["cfg_gray16_4k_step417"]
+    stream = fastvid_b200.encode(_cuda(case["make"]()), layout="gray", bit_depth=16, quality=87,
+                                 tile_size=(128, 128))
+    from fastvid_b200.codec import plan_decode
+
+    frame, _ = plan_decode(stream)
+    assert stream[7].item() == 0x88 and frame.step == 417 and frame.flags == 0x80
+
+
 def test_pitched_and_strided_planes_encode_like_contiguous(cuda):
     planes = synth.make_frame(301, 97, "rgb444", 10, 77)
     base = fastvid_b200.encode(_cuda(planes), layout="rgb444", bit_depth=10, quality=88, tile_size=(64, 32))

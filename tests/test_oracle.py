@@ -58,6 +58,14 @@ def test_oracle_matches_reference_golden(case):
         assert stored.read_bytes() == stream
 
 
+def test_reference_refined_config_3a_at_full_size():
+    """The reference's own 3840x2160 gray16 q87 stream is refined to step 417
+    (flag 0x80); the oracle's bytes for it are checked by the golden test."""
+    rec = RECORDS["cfg_gray16_4k_step417"]
+    assert rec["flags"] == 0x88
+    assert oracle.refined_gray16_step(87) == 417 and oracle.quantization_step("gray", 16, 87) == 556
+
+
 def _shard_modes(stream):
     """cuda/tests/test_codec.py:33-49"""
     tile_count = struct.unpack_from("<I", stream, 28)[0]
