@@ -61,6 +61,8 @@ SIGNATURES = {
     "fvb_get_launch_ctas": ([c_i32], c_i32),
     "fvb_set_wavefront_block": ([c_i32], c_i32),
     "fvb_get_wavefront_block": ([], c_i32),
+    "fvb_set_tile_warps": ([c_i32], c_i32),
+    "fvb_get_tile_warps": ([], c_i32),
     "fvb_profile_begin": ([], c_i32),
     "fvb_profile_end": ([c_p, c_p, c_i32], c_i32),
     "fvb_encode_plan": ([c_i64, c_i64, c_i32, c_i32, c_i32, c_i64, c_i64, c_i64, c_i64,

@@ -7,9 +7,11 @@ Three kinds of knob, tuned by measurement and kept in a JSON table:
   decode warps... share an SM.  No output byte depends on it.  Chosen by
   coordinate descent over the kernels on the measured encode+decode time of a
   sample batch.
-* Wavefront block -- how many of the 32 steps of each wavefront block the
-  predictor and reconstruction warps unroll (fvb_set_wavefront_block: 4, 8,
-  16 or 32).  No output byte depends on it; tuned before the launch caps.
+* Wavefront block and warps per tile -- how many of the 32 steps of each
+  wavefront block the predictor and reconstruction warps unroll
+  (fvb_set_wavefront_block: 4, 8, 16 or 32), and whether one warp or a warp
+  pair sweeps a tile's bands (fvb_set_tile_warps: 1 or 2).  No output byte
+  depends on either; tuned before the launch caps.
 * Tile geometry per frame format (layout, depth, width, height) -- the
   wavefront block each warp sweeps.  The tile size is written into the
   stream header, so it changes the bytes and the compression; the tuner takes
@@ -36,6 +38,7 @@ TABLE = Path(__file__).resolve().parent / "tuning" / "b200.json"
 LAUNCH_KNOBS = ("enc_predict", "enc_analyze", "enc_emit", "dec_rans", "dec_other", "dec_reconstruct")
 LAUNCH_CANDIDATES = (2, 3, 4, 6, 8, 12, 16)
 WAVEFRONT_BLOCKS = (4, 8, 16, 32)
+TILE_WARPS = (1, 2)
 TILE_CANDIDATES = ((32, 32), (64, 64), (128, 128))
 
 
@@ -111,10 +114,20 @@ def set_wavefront_block(steps: int) -> None:
     _native.check(_native.load().fvb_set_wavefront_block(int(steps)))
 
 
+def tile_warps() -> int:
+    return int(_native.load().fvb_get_tile_warps())
+
+
+def set_tile_warps(warps: int) -> None:
+    _native.check(_native.load().fvb_set_tile_warps(int(warps)))
+
+
 def apply(table: dict) -> None:
-    """Set the table's launch geometry and wavefront block (process-wide)."""
+    """Set the table's launch geometry, wavefront block and warps per tile
+    (process-wide)."""
     set_launch(table.get("launch", {}))
     set_wavefront_block(table.get("wavefront_block", 0))
+    set_tile_warps(table.get("tile_warps", 0))
 
 
 def tile_for(table: dict | None, layout: str, bit_depth: int, width: int, height: int, default=(256, 128)):
@@ -171,6 +184,17 @@ def tune_wavefront_block(codec, frames, params, candidates=WAVEFRONT_BLOCKS, rep
     return best, {str(k): round(v, 3) for k, v in seen.items()}
 
 
+def tune_tile_warps(codec, frames, params, candidates=TILE_WARPS, reps: int = 3) -> tuple[int, dict]:
+    """One warp or a warp pair per tile, whichever measures faster."""
+    seen = {}
+    for warps in candidates:
+        set_tile_warps(warps)
+        seen[warps] = _time_batch(codec, frames, params, reps)[0]
+    best = min(seen, key=seen.get)
+    set_tile_warps(best)
+    return best, {str(k): round(v, 3) for k, v in seen.items()}
+
+
 def tune_tiles(codec, groups: dict, candidates=TILE_CANDIDATES, size_tolerance: float = 0.02,
                reps: int = 3) -> tuple[dict, dict]:
     """groups: {format_key: (frames, params without tile_size)}.  Returns the
@@ -218,11 +242,13 @@ def main(argv=None) -> int:
                              for s in specs])
     base_ms = _time_batch(codec, frames, params, args.reps)[0]
     block, block_ms = tune_wavefront_block(codec, frames, params, reps=args.reps)
+    warps, warps_ms = tune_tile_warps(codec, frames, params, reps=args.reps)
     launch = tune_launch(codec, frames, params, reps=args.reps)
     tuned_ms = _time_batch(codec, frames, params, args.reps)[0]
     table = {"device": torch.cuda.get_device_name(dev), "sample": f"{args.frames}-frame mix",
              "size_tolerance": args.size_tolerance, "tiles": tiles, "tile_measurements_ms_bytes": measured,
              "wavefront_block": block, "wavefront_block_ms": block_ms,
+             "tile_warps": warps, "tile_warps_ms": warps_ms,
              "launch": launch, "launch_gain": {"default_ms": round(base_ms, 3), "tuned_ms": round(tuned_ms, 3)}}
     save(table, args.out)
     print(json.dumps(table))

@@ -578,6 +578,7 @@ constexpr int kDefaultCtas[K_COUNT] = {
     /*dec_rans*/ 16, /*dec_other*/ 16};
 std::atomic<int> g_ctas[K_COUNT];
 std::atomic<int> g_wavefront_block{kDefaultWavefrontBlock};
+std::atomic<int> g_tile_warps{kDefaultTileWarps};
 
 int ctas(int kernel) {
   const int v = g_ctas[kernel].load(std::memory_order_relaxed);
@@ -649,6 +650,15 @@ int fvb_set_wavefront_block(int steps) {
 }
 
 int fvb_get_wavefront_block(void) { return g_wavefront_block.load(std::memory_order_relaxed); }
+
+int fvb_set_tile_warps(int warps) {
+  if (warps == 0) warps = kDefaultTileWarps;
+  if (warps != 1 && warps != 2) return fail(FVB_ERR_ARGUMENT, "warps per tile must be 1 or 2");
+  g_tile_warps.store(warps, std::memory_order_relaxed);
+  return FVB_OK;
+}
+
+int fvb_get_tile_warps(void) { return g_tile_warps.load(std::memory_order_relaxed); }
 
 const char* fvb_kernel_name(int kernel) { return kernel >= 0 && kernel < K_COUNT ? kKernelNames[kernel] : ""; }
 
@@ -819,8 +829,9 @@ int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, 
     FVB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), stream));
     {
       LaunchScope scope_(K_ENC_PREDICT, stream);
-      enc_predict_launch(g_wavefront_block.load(std::memory_order_relaxed),
-                         grid_for(tiles, kWarpsPerCta, ctas(K_ENC_PREDICT)), stream, frames_d, state, dims, pass,
+      const int tw = g_tile_warps.load(std::memory_order_relaxed);
+      enc_predict_launch(g_wavefront_block.load(std::memory_order_relaxed), tw,
+                         grid_for(tiles * tw, kWarpsPerCta, ctas(K_ENC_PREDICT)), stream, frames_d, state, dims, pass,
                          shards, folded, queue);
     }
     FVB_LAUNCHED("enc_predict_kernel");
@@ -1198,9 +1209,10 @@ int decode_enqueue(const Totals& t, int wavefront, void* workspace, int64_t work
   if (wavefront) {
     {
       LaunchScope scope_(K_DEC_RECON, stream);
-      dec_reconstruct_launch(g_wavefront_block.load(std::memory_order_relaxed),
-                             grid_for(t.tiles, kWarpsPerCta, ctas(K_DEC_RECON)), stream, frames_d, state, dims, folded,
-                             queue);
+      const int tw = g_tile_warps.load(std::memory_order_relaxed);
+      dec_reconstruct_launch(g_wavefront_block.load(std::memory_order_relaxed), tw,
+                             grid_for(t.tiles * tw, kWarpsPerCta, ctas(K_DEC_RECON)), stream, frames_d, state, dims,
+                             folded, queue);
     }
     FVB_LAUNCHED("dec_reconstruct_kernel");
     if (t.wide) {

@@ -821,17 +821,20 @@ struct RecWarpSmem {
 
 size_t dec_reconstruct_smem() { return sizeof(RecWarpSmem) * kWarpsPerCta; }
 
-template <bool MED, bool STEP1, bool EDGE, int UNROLL>
-__device__ __forceinline__ void rec_block(RecWarpSmem& sm, int lane, int t0, int W, int32_t maxs, int32_t step,
-                                          bool band0, int32_t& rec, int32_t& a_prev) {
+template <bool MED, bool STEP1, bool EDGE, int UNROLL, bool SPLIT>
+__device__ __forceinline__ void rec_block(RecWarpSmem& sm, const uint16_t* carry_in, uint16_t* carry_out, int lane,
+                                          int t0, int W, int32_t maxs, int32_t step, bool band0, int32_t& rec,
+                                          int32_t& a_prev) {
   const uint32_t* frow = sm.fold + lane * kFoldStride + (t0 & 32);
   uint16_t* orow = sm.out + lane * kSrcStride + (t0 & 32);
-  uint16_t* crow = sm.carry + 32 - lane + t0;
+  const uint16_t* crow_in = carry_in + 32 - lane + t0;  // lane 0: column t0 + u
+  // one warp per tile reads and writes the same row: one pointer
+  uint16_t* crow_out = SPLIT ? carry_out + 32 - lane + t0 : const_cast<uint16_t*>(crow_in);      // lane 31: column t0 + u - 31
 #pragma unroll UNROLL
   for (int u = 0; u < 32; ++u) {
     const uint32_t fv = frow[u];
     int32_t a = __shfl_up_sync(0xffffffffu, rec, 1);
-    const int32_t above0 = crow[u];
+    const int32_t above0 = crow_in[u];
     if (lane == 0) a = band0 ? 0 : above0;
     const int32_t pred = MED ? predict_med(rec, a, a_prev) : predict_grad(rec, a, a_prev, maxs);
     const int32_t q = unzigzag(fv);
@@ -839,9 +842,9 @@ __device__ __forceinline__ void rec_block(RecWarpSmem& sm, int lane, int t0, int
     if (EDGE) {
       const int c = t0 + u - lane;
       if (c < 0) rn = 0;
-      if (lane == 31 && c >= 0 && c < W) crow[u] = static_cast<uint16_t>(rn);
+      if (lane == 31 && c >= 0 && c < W) crow_out[u] = static_cast<uint16_t>(rn);
     } else {
-      if (lane == 31) crow[u] = static_cast<uint16_t>(rn);
+      if (lane == 31) crow_out[u] = static_cast<uint16_t>(rn);
     }
     orow[u] = static_cast<uint16_t>(rn);
     a_prev = a;
@@ -849,85 +852,170 @@ __device__ __forceinline__ void rec_block(RecWarpSmem& sm, int lane, int t0, int
   }
 }
 
-template <bool MED, bool STEP1, int UNROLL>
-__device__ void rec_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step,
-                              const uint32_t* __restrict__ ftile, RecWarpSmem& sm, int lane) {
-  uint16_t* __restrict__ plane = f.dst[g.plane];
-  const int64_t pitch = f.dst_pitch[g.plane];
-  const int W = g.w, H = g.h;
-  const int32_t maxs = f.max_sample;
-  const int nchunks = (W + 31) >> 5;
-  const int nblocks = (W + 31 + 31) >> 5;
-  for (int band = 0; band * 32 < H; ++band) {
-    const int band_rows = min(32, H - band * 32);
-    uint16_t* __restrict__ orows = plane + static_cast<int64_t>(g.y + band * 32) * pitch + g.x;
-    const uint32_t* __restrict__ frows = ftile + static_cast<int64_t>(band * 32) * W;
-    uint32_t pf[32];
-    auto load_chunk = [&](int k) {
-      const int col = k * 32 + lane;
-      const uint32_t* __restrict__ p = frows + col;
-      if (band_rows == 32 && col < W) {
+// One warp's sweep of one 32-row band of a tile, block by block: begin()
+// stages the first folded chunks, block(k) runs wavefront block k (staging
+// the chunk ahead and flushing the reconstruction two chunks behind), end()
+// flushes the rest.  Lane 0 reads the row above the band from carry_in;
+// lane 31 writes the band's last row to carry_out (one warp per tile: the
+// same row, read before it is overwritten).
+template <bool MED, bool STEP1, int UNROLL, bool SPLIT>
+struct RecBand {
+  RecWarpSmem& sm;
+  int lane;
+  uint16_t* __restrict__ plane;
+  int64_t pitch;
+  int W, H, x0, y0;
+  int32_t maxs, step;
+  int nchunks, nblocks;
+  const uint32_t* __restrict__ ftile;
+  int band_rows;
+  bool band0;
+  uint16_t* __restrict__ orows;
+  const uint32_t* __restrict__ frows;
+  const uint16_t* carry_in;
+  uint16_t* carry_out;
+  int32_t rec, a_prev;
+  uint32_t pf[32];
+
+  __device__ RecBand(const FrameDesc& f, const TileGeo& g, int32_t step_, const uint32_t* ftile_, RecWarpSmem& sm_,
+                     int lane_)
+      : sm(sm_), lane(lane_), plane(f.dst[g.plane]), pitch(f.dst_pitch[g.plane]), W(g.w), H(g.h), x0(g.x),
+        y0(g.y), maxs(f.max_sample), step(step_), nchunks((g.w + 31) >> 5), nblocks((g.w + 31 + 31) >> 5),
+        ftile(ftile_) {}
+
+  __device__ void load_chunk(int k) {
+    const int col = k * 32 + lane;
+    const uint32_t* __restrict__ p = frows + col;
+    if (band_rows == 32 && col < W) {
 #pragma unroll
-        for (int r = 0; r < 32; ++r) pf[r] = __ldg(p + static_cast<int64_t>(r) * W);
+      for (int r = 0; r < 32; ++r) pf[r] = __ldg(p + static_cast<int64_t>(r) * W);
+    } else {
+#pragma unroll
+      for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && col < W) ? __ldg(p + static_cast<int64_t>(r) * W) : 0u;
+    }
+  }
+  __device__ void store_chunk(int k) {
+    const int pj = k * 32 + lane;
+#pragma unroll
+    for (int r = 0; r < 32; ++r) sm.fold[r * kFoldStride + ((pj + r) & 63)] = pf[r];
+  }
+  __device__ void flush_chunk(int k) {
+    const int col = k * 32 + lane;
+    if (col < W) {
+      uint16_t* __restrict__ q = orows + col;
+      if (band_rows == 32) {
+#pragma unroll
+        for (int r = 0; r < 32; ++r) q[static_cast<int64_t>(r) * pitch] = sm.out[r * kSrcStride + ((col + r) & 63)];
       } else {
-#pragma unroll
-        for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && col < W) ? __ldg(p + static_cast<int64_t>(r) * W) : 0u;
+        for (int r = 0; r < band_rows; ++r) q[static_cast<int64_t>(r) * pitch] = sm.out[r * kSrcStride + ((col + r) & 63)];
       }
-    };
-    auto store_chunk = [&](int k) {
-      const int pj = k * 32 + lane;
-#pragma unroll
-      for (int r = 0; r < 32; ++r) sm.fold[r * kFoldStride + ((pj + r) & 63)] = pf[r];
-    };
-    auto flush_chunk = [&](int k) {
-      const int col = k * 32 + lane;
-      if (col < W) {
-        uint16_t* __restrict__ q = orows + col;
-        if (band_rows == 32) {
-#pragma unroll
-          for (int r = 0; r < 32; ++r) q[static_cast<int64_t>(r) * pitch] = sm.out[r * kSrcStride + ((col + r) & 63)];
-        } else {
-          for (int r = 0; r < band_rows; ++r) q[static_cast<int64_t>(r) * pitch] = sm.out[r * kSrcStride + ((col + r) & 63)];
-        }
-      }
-    };
+    }
+  }
+  __device__ void begin(int band, const uint16_t* cin, uint16_t* cout) {
+    band_rows = min(32, H - band * 32);
+    band0 = band == 0;
+    orows = plane + static_cast<int64_t>(y0 + band * 32) * pitch + x0;
+    frows = ftile + static_cast<int64_t>(band * 32) * W;
+    carry_in = cin;
+    carry_out = cout;
     load_chunk(0);
     store_chunk(0);
     if (nchunks > 1) load_chunk(1);
     __syncwarp();
-    int32_t rec = 0, a_prev = 0;
-    const bool band0 = band == 0;
-    for (int blk = 0; blk < nblocks; ++blk) {
-      if (blk > 0) {
-        if (blk < nchunks) store_chunk(blk);
-        __syncwarp();
-        if (blk >= 2 && blk - 2 < nchunks) flush_chunk(blk - 2);
-        if (blk + 1 < nchunks) load_chunk(blk + 1);
-      }
-      const int t0 = blk * 32;
-      if (t0 < 31 || t0 + 31 >= W) rec_block<MED, STEP1, true, UNROLL>(sm, lane, t0, W, maxs, step, band0, rec, a_prev);
-      else rec_block<MED, STEP1, false, UNROLL>(sm, lane, t0, W, maxs, step, band0, rec, a_prev);
+    rec = 0;
+    a_prev = 0;
+  }
+  __device__ void block(int blk) {
+    if (blk > 0) {
+      if (blk < nchunks) store_chunk(blk);
+      __syncwarp();
+      if (blk >= 2 && blk - 2 < nchunks) flush_chunk(blk - 2);
+      if (blk + 1 < nchunks) load_chunk(blk + 1);
     }
+    const int t0 = blk * 32;
+    if (t0 < 31 || t0 + 31 >= W)
+      rec_block<MED, STEP1, true, UNROLL, SPLIT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, band0, rec, a_prev);
+    else
+      rec_block<MED, STEP1, false, UNROLL, SPLIT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, band0, rec, a_prev);
+  }
+  __device__ void end() {
     __syncwarp();
     for (int j = max(0, nblocks - 2); j < nchunks; ++j) flush_chunk(j);
     __syncwarp();
   }
+};
+
+// The two warps of pair p meet at named barrier 1 + p (64 threads).
+__device__ __forceinline__ void pair_sync(int pair) {
+  asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");
 }
 
-template <int UNROLL>
-__global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
+template <bool MED, bool STEP1, int UNROLL, bool PAIRS>
+__device__ void rec_tile(const FrameDesc& f, const TileGeo& g, int32_t step, const uint32_t* __restrict__ ftile,
+                         RecWarpSmem* smw, int warp, int lane) {
+  if constexpr (PAIRS) {
+    if (pair_splits(g.w, g.h)) {
+      // warp pair: even bands on the first warp, odd bands on the second two
+      // blocks behind, in lock-step at the pair barrier after every slot; each
+      // warp writes its bands' last rows to its own carry row and reads the
+      // other's.  Both warps take the same number of slots (a function of the
+      // tile's size only).
+      const int pw = warp & 1;
+      RecWarpSmem& sm = smw[warp];
+      RecBand<MED, STEP1, UNROLL, true> rb(f, g, step, ftile, sm, lane);
+      const int n = rb.nblocks, nbands = (g.h + 31) >> 5;
+      const int own = pw ? (nbands / 2) * n : ((nbands + 1) / 2) * n;
+      const int slots = max(((nbands + 1) / 2) * n, (nbands / 2) * n + 2);
+      for (int gs = 0; gs < slots; ++gs) {
+        const int sl = gs - 2 * pw;
+        if (sl >= 0 && sl < own) {
+          const int q = sl / n, blk = sl - q * n;
+          if (blk == 0) rb.begin(2 * q + pw, smw[warp ^ 1].carry, sm.carry);
+          rb.block(blk);
+          if (blk == n - 1) rb.end();
+        }
+        pair_sync(warp >> 1);
+      }
+      return;
+    }
+    if (warp & 1) return;  // too small to split: the pair's first warp alone
+  }
+  RecWarpSmem& sm = smw[warp];
+  RecBand<MED, STEP1, UNROLL, false> rb(f, g, step, ftile, sm, lane);
+  for (int band = 0; band * 32 < g.h; ++band) {
+    rb.begin(band, sm.carry, sm.carry);
+    for (int blk = 0; blk < rb.nblocks; ++blk) rb.block(blk);
+    rb.end();
+  }
+}
+
+// Tiles come from a queue.  With warp pairs, the pair's first warp claims a
+// tile and both read it after the pair barrier (two alternating slots, so a
+// claim never overwrites a tile the other warp has yet to read); both then
+// make the same decisions from the same tile, so they meet at every barrier.
+template <int UNROLL, bool PAIRS>
+__global__ void __launch_bounds__(kWarpsPerCta * 32, PAIRS ? 3 : 4)
 dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
                        const BatchDims* __restrict__ dims, const uint32_t* __restrict__ folded,
                        int* __restrict__ queue) {
+  static_assert(kWarpsPerCta % 2 == 0, "warp pairs");
+  constexpr bool pairs = PAIRS;
   const int nframes = dims->frames_p[0];
   const int64_t total_tiles = dims->tiles_p[0];
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int64_t claimed[kWarpsPerCta / 2][2];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  RecWarpSmem& sm = reinterpret_cast<RecWarpSmem*>(smem_raw)[warp];
-  for (;;) {
+  RecWarpSmem* smw = reinterpret_cast<RecWarpSmem*>(smem_raw);
+  for (int it = 0;; ++it) {
     int64_t t = 0;
-    if (lane == 0) t = atomicAdd(queue, 1);
-    t = __shfl_sync(kFull, t, 0);
+    if (pairs) {
+      if ((warp & 1) == 0 && lane == 0) claimed[warp >> 1][it & 1] = atomicAdd(queue, 1);
+      pair_sync(warp >> 1);
+      t = claimed[warp >> 1][it & 1];
+    } else {
+      if (lane == 0) t = atomicAdd(queue, 1);
+      t = __shfl_sync(kFull, t, 0);
+    }
     if (t >= total_tiles) break;
     const int fi = frame_of_tile(frames, nframes, t);
     const FrameDesc& f = frames[fi];
@@ -936,11 +1024,11 @@ dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* _
     if (g.w > kFastMaxW) continue;
     const uint32_t* ftile = folded + f.sample_base + g.sample_base;
     if (f.use_med0) {
-      if (f.step0 == 1) rec_tile_fast<true, true, UNROLL>(f, g, 1, ftile, sm, lane);
-      else rec_tile_fast<true, false, UNROLL>(f, g, f.step0, ftile, sm, lane);
+      if (f.step0 == 1) rec_tile<true, true, UNROLL, PAIRS>(f, g, 1, ftile, smw, warp, lane);
+      else rec_tile<true, false, UNROLL, PAIRS>(f, g, f.step0, ftile, smw, warp, lane);
     } else {
-      if (f.step0 == 1) rec_tile_fast<false, true, UNROLL>(f, g, 1, ftile, sm, lane);
-      else rec_tile_fast<false, false, UNROLL>(f, g, f.step0, ftile, sm, lane);
+      if (f.step0 == 1) rec_tile<false, true, UNROLL, PAIRS>(f, g, 1, ftile, smw, warp, lane);
+      else rec_tile<false, false, UNROLL, PAIRS>(f, g, f.step0, ftile, smw, warp, lane);
     }
   }
 }
@@ -949,20 +1037,22 @@ dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* _
 // enc_predict (4, 8, 16 or 32 steps unrolled; identical planes).
 cudaError_t dec_reconstruct_set_smem() {
   const int bytes = static_cast<int>(dec_reconstruct_smem());
-  for (auto k : {dec_reconstruct_kernel<4>, dec_reconstruct_kernel<8>, dec_reconstruct_kernel<16>,
-                 dec_reconstruct_kernel<32>}) {
+  for (auto k : {dec_reconstruct_kernel<4, false>, dec_reconstruct_kernel<8, false>, dec_reconstruct_kernel<16, false>,
+                 dec_reconstruct_kernel<32, false>, dec_reconstruct_kernel<8, true>}) {
     const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
 
-void dec_reconstruct_launch(int unroll, int grid, cudaStream_t stream, const FrameDesc* frames,
+void dec_reconstruct_launch(int unroll, int tile_warps, int grid, cudaStream_t stream, const FrameDesc* frames,
                             const FrameState* state, const BatchDims* dims, const uint32_t* folded, int* queue) {
-  auto k = unroll == 4    ? dec_reconstruct_kernel<4>
-           : unroll == 16 ? dec_reconstruct_kernel<16>
-           : unroll == 32 ? dec_reconstruct_kernel<32>
-                          : dec_reconstruct_kernel<8>;
+  // warp pairs run with the default wavefront block
+  auto k = tile_warps == 2 ? dec_reconstruct_kernel<8, true>
+           : unroll == 4   ? dec_reconstruct_kernel<4, false>
+           : unroll == 16  ? dec_reconstruct_kernel<16, false>
+           : unroll == 32  ? dec_reconstruct_kernel<32, false>
+                           : dec_reconstruct_kernel<8, false>;
   k<<<grid, kWarpsPerCta * 32, dec_reconstruct_smem(), stream>>>(frames, state, dims, folded, queue);
 }
 

@@ -59,18 +59,20 @@ struct EncWarpSmem {
   uint16_t carry[kFastMaxW + 128];  // row above the band, column c at index c + 32
 };
 
-template <bool MED, bool STEP1, bool EDGE, int UNROLL>
-__device__ __forceinline__ void enc_block(EncWarpSmem& sm, int lane, int t0, int W,
-                                          int32_t maxs, int32_t step, int32_t half, uint32_t magic, bool band0,
-                                          int32_t& rec, int32_t& a_prev) {
+template <bool MED, bool STEP1, bool EDGE, int UNROLL, bool SPLIT>
+__device__ __forceinline__ void enc_block(EncWarpSmem& sm, const uint16_t* carry_in, uint16_t* carry_out, int lane,
+                                          int t0, int W, int32_t maxs, int32_t step, int32_t half, uint32_t magic,
+                                          bool band0, int32_t& rec, int32_t& a_prev) {
   const uint16_t* srow = sm.src + lane * kSrcStride + (t0 & 32);
   uint32_t* frow = sm.fold + lane * kFoldStride + (t0 & 32);
-  uint16_t* crow = sm.carry + 32 - lane + t0;  // carry index (t - lane) + 32
+  const uint16_t* crow_in = carry_in + 32 - lane + t0;  // lane 0: column t0 + u
+  // one warp per tile reads and writes the same row: one pointer
+  uint16_t* crow_out = SPLIT ? carry_out + 32 - lane + t0 : const_cast<uint16_t*>(crow_in);      // lane 31: column t0 + u - 31 (index (t - lane) + 32)
 #pragma unroll UNROLL
   for (int u = 0; u < 32; ++u) {
     const int32_t s = srow[u];
     int32_t a = __shfl_up_sync(0xffffffffu, rec, 1);
-    const int32_t above0 = crow[u];
+    const int32_t above0 = crow_in[u];
     if (lane == 0) a = band0 ? 0 : above0;
     const int32_t pred = MED ? predict_med(rec, a, a_prev) : predict_grad(rec, a, a_prev, maxs);
     const int32_t res = s - pred;
@@ -86,9 +88,9 @@ __device__ __forceinline__ void enc_block(EncWarpSmem& sm, int lane, int t0, int
     if (EDGE) {
       const int c = t0 + u - lane;
       if (c < 0) rn = 0;  // left of the tile: zero left/upper-left for column 0
-      if (lane == 31 && c >= 0 && c < W) crow[u] = static_cast<uint16_t>(rn);
+      if (lane == 31 && c >= 0 && c < W) crow_out[u] = static_cast<uint16_t>(rn);
     } else {
-      if (lane == 31) crow[u] = static_cast<uint16_t>(rn);
+      if (lane == 31) crow_out[u] = static_cast<uint16_t>(rn);
     }
     frow[u] = zigzag(q);
     a_prev = a;
@@ -96,6 +98,107 @@ __device__ __forceinline__ void enc_block(EncWarpSmem& sm, int lane, int t0, int
   }
 }
 
+// One warp's sweep of one 32-row band of a tile, block by block (the
+// encoder's mirror of the decoder's RecBand): begin() stages the first
+// source chunks, block(k) runs wavefront block k (staging the chunk ahead
+// and flushing the folded residuals two chunks behind), end() flushes the
+// rest.  vmax tracks the largest source sample read (the depth check).
+template <bool MED, bool STEP1, int UNROLL, bool SPLIT>
+struct EncBand {
+  EncWarpSmem& sm;
+  int lane;
+  const uint16_t* __restrict__ plane;
+  int64_t pitch;
+  int W, H, x0, y0;
+  int32_t maxs, step, half;
+  uint32_t magic;
+  int nchunks, nblocks;
+  uint32_t* __restrict__ ftile;
+  uint32_t vmax = 0;
+  int band_rows;
+  bool band0;
+  const uint16_t* __restrict__ rows;
+  uint32_t* __restrict__ frows;
+  const uint16_t* carry_in;
+  uint16_t* carry_out;
+  int32_t rec, a_prev;
+  uint32_t pf[32];
+
+  __device__ EncBand(const FrameDesc& f, const TileGeo& g, int32_t step_, uint32_t magic_, uint32_t* ftile_,
+                     EncWarpSmem& sm_, int lane_)
+      : sm(sm_), lane(lane_), plane(f.src[g.plane]), pitch(f.src_pitch[g.plane]), W(g.w), H(g.h), x0(g.x), y0(g.y),
+        maxs(f.max_sample), step(step_), half(step_ >> 1), magic(magic_), nchunks((g.w + 31) >> 5),
+        nblocks((g.w + 31 + 31) >> 5), ftile(ftile_) {}
+
+  __device__ void load_chunk(int k) {
+    const int col = k * 32 + lane;
+    const uint16_t* __restrict__ p = rows + col;
+    if (band_rows == 32 && col < W) {
+#pragma unroll
+      for (int r = 0; r < 32; ++r) pf[r] = __ldg(p + static_cast<int64_t>(r) * pitch);
+    } else {
+#pragma unroll
+      for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && col < W) ? __ldg(p + static_cast<int64_t>(r) * pitch) : 0u;
+    }
+#pragma unroll
+    for (int r = 0; r < 32; ++r) vmax = max(vmax, pf[r]);
+  }
+  __device__ void store_chunk(int k) {
+    const int pj = k * 32 + lane;
+#pragma unroll
+    for (int r = 0; r < 32; ++r) sm.src[r * kSrcStride + ((pj + r) & 63)] = static_cast<uint16_t>(pf[r]);
+  }
+  __device__ void flush_chunk(int k) {
+    const int col = k * 32 + lane;
+    if (col < W) {
+      uint32_t* __restrict__ q = frows + col;
+      if (band_rows == 32) {
+#pragma unroll
+        for (int r = 0; r < 32; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFoldStride + ((col + r) & 63)];
+      } else {
+        for (int r = 0; r < band_rows; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFoldStride + ((col + r) & 63)];
+      }
+    }
+  }
+  __device__ void begin(int band, const uint16_t* cin, uint16_t* cout) {
+    band_rows = min(32, H - band * 32);
+    band0 = band == 0;
+    rows = plane + static_cast<int64_t>(y0 + band * 32) * pitch + x0;
+    frows = ftile + static_cast<int64_t>(band * 32) * W;
+    carry_in = cin;
+    carry_out = cout;
+    load_chunk(0);
+    store_chunk(0);
+    if (nchunks > 1) load_chunk(1);
+    __syncwarp();
+    rec = 0;
+    a_prev = 0;
+  }
+  __device__ void block(int blk) {
+    if (blk > 0) {
+      if (blk < nchunks) store_chunk(blk);
+      __syncwarp();
+      if (blk >= 2 && blk - 2 < nchunks) flush_chunk(blk - 2);
+      if (blk + 1 < nchunks) load_chunk(blk + 1);
+    }
+    const int t0 = blk * 32;
+    if (t0 < 31 || t0 + 31 >= W)
+      enc_block<MED, STEP1, true, UNROLL, SPLIT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, half, magic, band0, rec,
+                                          a_prev);
+    else
+      enc_block<MED, STEP1, false, UNROLL, SPLIT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, half, magic, band0, rec,
+                                           a_prev);
+  }
+  __device__ void end() {
+    __syncwarp();
+    for (int j = max(0, nblocks - 2); j < nchunks; ++j) flush_chunk(j);
+    __syncwarp();
+  }
+};
+
+// A tile by one warp: bands in order, one carry row (read by lane 0 before
+// lane 31 overwrites it).  Kept apart from EncBand: written as one loop nest
+// it needs no register spills.
 template <bool MED, bool STEP1, int UNROLL>
 __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step, uint32_t magic,
                               uint32_t* __restrict__ folded_tile, EncWarpSmem& sm, int lane, int32_t& bad) {
@@ -157,8 +260,12 @@ __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
       }
       const int t0 = blk * 32;
       const bool edge = t0 < 31 || t0 + 31 >= W;
-      if (edge) enc_block<MED, STEP1, true, UNROLL>(sm, lane, t0, W, maxs, step, half, magic, band0, rec, a_prev);
-      else enc_block<MED, STEP1, false, UNROLL>(sm, lane, t0, W, maxs, step, half, magic, band0, rec, a_prev);
+      if (edge)
+        enc_block<MED, STEP1, true, UNROLL, false>(sm, sm.carry, sm.carry, lane, t0, W, maxs, step, half, magic, band0,
+                                                   rec, a_prev);
+      else
+        enc_block<MED, STEP1, false, UNROLL, false>(sm, sm.carry, sm.carry, lane, t0, W, maxs, step, half, magic,
+                                                    band0, rec, a_prev);
     }
     __syncwarp();
     for (int j = max(0, nblocks - 2); j < nchunks; ++j) flush_chunk(j);
@@ -167,33 +274,85 @@ __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
   if (vmax > static_cast<uint32_t>(maxs)) bad = 1;
 }
 
-template <int UNROLL>
-__global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
+// The two warps of pair p meet at named barrier 1 + p (64 threads).
+__device__ __forceinline__ void enc_pair_sync(int pair) {
+  asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");
+}
+
+template <bool MED, bool STEP1, int UNROLL, bool PAIRS>
+__device__ void enc_tile(const FrameDesc& f, const TileGeo& g, int32_t step, uint32_t magic,
+                         uint32_t* __restrict__ folded_tile, EncWarpSmem* smw, int warp, int lane, int32_t& bad) {
+  if constexpr (PAIRS) {
+    if (pair_splits(g.w, g.h)) {
+      // warp pair: even bands on the first warp, odd bands on the second two
+      // blocks behind, in lock-step at the pair barrier after every slot (the
+      // schedule of dec_reconstruct)
+      const int pw = warp & 1;
+      EncWarpSmem& sm = smw[warp];
+      EncBand<MED, STEP1, UNROLL, true> eb(f, g, step, magic, folded_tile, sm, lane);
+      const int n = eb.nblocks, nbands = (g.h + 31) >> 5;
+      const int own = pw ? (nbands / 2) * n : ((nbands + 1) / 2) * n;
+      const int slots = max(((nbands + 1) / 2) * n, (nbands / 2) * n + 2);
+      for (int gs = 0; gs < slots; ++gs) {
+        const int sl = gs - 2 * pw;
+        if (sl >= 0 && sl < own) {
+          const int q = sl / n, blk = sl - q * n;
+          if (blk == 0) eb.begin(2 * q + pw, smw[warp ^ 1].carry, sm.carry);
+          eb.block(blk);
+          if (blk == n - 1) eb.end();
+        }
+        enc_pair_sync(warp >> 1);
+      }
+      if (eb.vmax > static_cast<uint32_t>(f.max_sample)) bad = 1;
+      return;
+    }
+    if (warp & 1) return;  // too small to split: the pair's first warp alone
+  }
+  enc_tile_fast<MED, STEP1, UNROLL>(f, g, step, magic, folded_tile, smw[warp], lane, bad);
+}
+
+// Tiles come from a queue; with warp pairs the pair's first warp claims a
+// tile and both read it after the pair barrier (two alternating slots), and
+// both make the same decisions from it, so they meet at every barrier.
+template <int UNROLL, bool PAIRS>
+__global__ void __launch_bounds__(kWarpsPerCta * 32, PAIRS ? 3 : 4)
 enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
                    const BatchDims* __restrict__ dims, int pass, ShardInfo* __restrict__ shards,
                    uint32_t* __restrict__ folded, int* __restrict__ queue) {
+  static_assert(kWarpsPerCta % 2 == 0, "warp pairs");
+  constexpr bool pairs = PAIRS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int64_t claimed[kWarpsPerCta / 2][2];
   const int nframes = dims->frames_p[pass];
   const int64_t total_tiles = dims->tiles_p[pass];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  EncWarpSmem& sm = reinterpret_cast<EncWarpSmem*>(smem_raw)[warp];
-  for (;;) {
+  EncWarpSmem* smw = reinterpret_cast<EncWarpSmem*>(smem_raw);
+  for (int it = 0;; ++it) {
     int64_t t = 0;
-    if (lane == 0) t = atomicAdd(queue, 1);
-    t = __shfl_sync(kFull, t, 0);
+    if (pairs) {
+      if ((warp & 1) == 0 && lane == 0) claimed[warp >> 1][it & 1] = atomicAdd(queue, 1);
+      enc_pair_sync(warp >> 1);
+      t = claimed[warp >> 1][it & 1];
+    } else {
+      if (lane == 0) t = atomicAdd(queue, 1);
+      t = __shfl_sync(kFull, t, 0);
+    }
     if (t >= total_tiles) break;
     const int fi = frame_of_tile(frames, nframes, t);
     const FrameDesc& f = frames[fi];
     FrameState& st = state[fi];
     if (!st.active) continue;
     const TileGeo g = tile_geo(f, t - f.tile_base);
-    // shard records of this tile (encode.cu:753-759)
-    for (int j = lane; j < g.shard_count; j += 32) {
-      ShardInfo& si = shards[f.shard_base + g.first_shard + j];
-      const int64_t local = static_cast<int64_t>(j) * kShardSymbols;
-      si.sample_base = f.sample_base + g.sample_base + local;
-      si.count = static_cast<int32_t>(min(static_cast<int64_t>(kShardSymbols), static_cast<int64_t>(g.w) * g.h - local));
-      si.frame = fi;
+    // shard records of this tile (encode.cu:753-759); with pairs the first
+    // warp writes them
+    if (!pairs || (warp & 1) == 0) {
+      for (int j = lane; j < g.shard_count; j += 32) {
+        ShardInfo& si = shards[f.shard_base + g.first_shard + j];
+        const int64_t local = static_cast<int64_t>(j) * kShardSymbols;
+        si.sample_base = f.sample_base + g.sample_base + local;
+        si.count = static_cast<int32_t>(min(static_cast<int64_t>(kShardSymbols), static_cast<int64_t>(g.w) * g.h - local));
+        si.frame = fi;
+      }
     }
     if (g.w > kFastMaxW) continue;  // wide tiles go through enc_predict_wide_kernel
     const int32_t step = st.step;
@@ -202,11 +361,11 @@ enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     int32_t bad = 0;
     const bool med = st.use_med != 0;
     if (med) {
-      if (step == 1) enc_tile_fast<true, true, UNROLL>(f, g, step, magic, ftile, sm, lane, bad);
-      else enc_tile_fast<true, false, UNROLL>(f, g, step, magic, ftile, sm, lane, bad);
+      if (step == 1) enc_tile<true, true, UNROLL, PAIRS>(f, g, step, magic, ftile, smw, warp, lane, bad);
+      else enc_tile<true, false, UNROLL, PAIRS>(f, g, step, magic, ftile, smw, warp, lane, bad);
     } else {
-      if (step == 1) enc_tile_fast<false, true, UNROLL>(f, g, step, magic, ftile, sm, lane, bad);
-      else enc_tile_fast<false, false, UNROLL>(f, g, step, magic, ftile, sm, lane, bad);
+      if (step == 1) enc_tile<false, true, UNROLL, PAIRS>(f, g, step, magic, ftile, smw, warp, lane, bad);
+      else enc_tile<false, false, UNROLL, PAIRS>(f, g, step, magic, ftile, smw, warp, lane, bad);
     }
     if (__any_sync(kFull, bad) && lane == 0) set_status(&st.status, 1);
   }
@@ -217,19 +376,23 @@ enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
 // choice computes the same bytes.
 cudaError_t enc_predict_set_smem() {
   const int bytes = static_cast<int>(enc_predict_smem());
-  for (auto k : {enc_predict_kernel<4>, enc_predict_kernel<8>, enc_predict_kernel<16>, enc_predict_kernel<32>}) {
+  for (auto k : {enc_predict_kernel<4, false>, enc_predict_kernel<8, false>, enc_predict_kernel<16, false>,
+                 enc_predict_kernel<32, false>, enc_predict_kernel<8, true>}) {
     const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
 
-void enc_predict_launch(int unroll, int grid, cudaStream_t stream, const FrameDesc* frames, FrameState* state,
-                        const BatchDims* dims, int pass, ShardInfo* shards, uint32_t* folded, int* queue) {
-  auto k = unroll == 4    ? enc_predict_kernel<4>
-           : unroll == 16 ? enc_predict_kernel<16>
-           : unroll == 32 ? enc_predict_kernel<32>
-                          : enc_predict_kernel<8>;
+void enc_predict_launch(int unroll, int tile_warps, int grid, cudaStream_t stream, const FrameDesc* frames,
+                        FrameState* state, const BatchDims* dims, int pass, ShardInfo* shards, uint32_t* folded,
+                        int* queue) {
+  // warp pairs run with the default wavefront block
+  auto k = tile_warps == 2 ? enc_predict_kernel<8, true>
+           : unroll == 4   ? enc_predict_kernel<4, false>
+           : unroll == 16  ? enc_predict_kernel<16, false>
+           : unroll == 32  ? enc_predict_kernel<32, false>
+                           : enc_predict_kernel<8, false>;
   k<<<grid, kWarpsPerCta * 32, enc_predict_smem(), stream>>>(frames, state, dims, pass, shards, folded, queue);
 }
 

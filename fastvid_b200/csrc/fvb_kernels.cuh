@@ -11,12 +11,22 @@ constexpr int kSrcStride = 66;     // u16 ring row stride: 64 columns + 2 (33 wo
 constexpr int kFoldStride = 65;    // u32 ring row stride: 64 columns + 1 (conflict-free)
 constexpr int kFastMaxW = 512;     // widest tile of the register-wavefront path
 constexpr int kDefaultWavefrontBlock = 8;  // steps of a 32-step wavefront block unrolled (4, 8, 16, 32)
+constexpr int kDefaultTileWarps = 1;       // warps per tile of the wavefront kernels (1 or 2)
+
+// Whether a warp pair splits a tile's bands (the predictor and the
+// reconstruction alike): at least two bands, and at least four wavefront
+// blocks per band -- the second warp runs two blocks behind the first, and
+// the band below needs the band above's last row up to one block ahead of
+// it, which the schedule provides once a band has four blocks.
+__host__ __device__ inline bool pair_splits(int w, int h) { return ((h + 31) >> 5) >= 2 && ((w + 62) >> 5) >= 4; }
 
 // encoder (counts of pass `pass` from dims)
 __global__ void enc_init_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims);
 // enc_predict with a wavefront block of `unroll` steps (4, 8, 16, 32)
-void enc_predict_launch(int unroll, int grid, cudaStream_t stream, const FrameDesc* frames, FrameState* state,
-                        const BatchDims* dims, int pass, ShardInfo* shards, uint32_t* folded, int* queue);
+// and `tile_warps` (1, or 2: a warp pair splits each tile's bands)
+void enc_predict_launch(int unroll, int tile_warps, int grid, cudaStream_t stream, const FrameDesc* frames,
+                        FrameState* state, const BatchDims* dims, int pass, ShardInfo* shards, uint32_t* folded,
+                        int* queue);
 cudaError_t enc_predict_set_smem();
 __global__ void enc_predict_wide_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
                                         uint32_t* folded, uint16_t* recon);
@@ -51,7 +61,7 @@ __global__ void dec_rans_kernel(const FrameDesc* frames, FrameState* state, cons
 __global__ void dec_other_kernel(const FrameDesc* frames, FrameState* state, const ShardInfo* shards,
                                  const BatchDims* dims, DecodeLists* lists, const int32_t* list_items,
                                  uint32_t* folded);
-void dec_reconstruct_launch(int unroll, int grid, cudaStream_t stream, const FrameDesc* frames,
+void dec_reconstruct_launch(int unroll, int tile_warps, int grid, cudaStream_t stream, const FrameDesc* frames,
                             const FrameState* state, const BatchDims* dims, const uint32_t* folded, int* queue);
 cudaError_t dec_reconstruct_set_smem();
 __global__ void dec_reconstruct_wide_kernel(const FrameDesc* frames, const FrameState* state, const BatchDims* dims,

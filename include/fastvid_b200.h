@@ -83,6 +83,14 @@ int fvb_get_launch_ctas(int kernel);
  * depends on it (the autotuner's knob). */
 int fvb_set_wavefront_block(int steps);
 int fvb_get_wavefront_block(void);
+/* Warps per tile of the predictor and reconstruction kernels (no reference
+ * counterpart; the autotuner's knob): 1, or 2 -- a warp pair sweeps a tile's
+ * even and odd 32-row bands in lock-step, the second warp two blocks behind,
+ * handing each band's last row over in shared memory (tiles of one band or
+ * under 66 columns stay on one warp).  0 restores the default (1).
+ * Process-wide, read at each launch; no output depends on it. */
+int fvb_set_tile_warps(int warps);
+int fvb_get_tile_warps(void);
 /* While profiling is on (per calling thread), every launch is bracketed by
  * CUDA events on its stream; fvb_profile_end waits for them and writes, per
  * kernel id, the summed milliseconds and the number of launches. */

@@ -84,3 +84,21 @@ def test_wavefront_block_knob_round_trip_and_rejections():
         assert autotune.wavefront_block() == 16
     finally:
         autotune.set_wavefront_block(before)
+
+
+def test_tile_warps_knob_round_trip_and_rejections():
+    lib = _native.load()
+    before = autotune.tile_warps()
+    try:
+        for warps in autotune.TILE_WARPS:
+            autotune.set_tile_warps(warps)
+            assert autotune.tile_warps() == warps
+        for bad in (3, 4, -1):
+            assert lib.fvb_set_tile_warps(bad) == -1
+            assert "warps per tile" in _native.last_error()
+        autotune.set_tile_warps(0)
+        assert autotune.tile_warps() == 1  # the default
+        autotune.apply({"launch": {}, "tile_warps": 2})
+        assert autotune.tile_warps() == 2
+    finally:
+        autotune.set_tile_warps(before)

@@ -180,3 +180,34 @@ def test_host_round_trip_matches_device_batch(cuda, mixed):
         assert not st.is_cuda and bytes(st.numpy().tobytes()) == f["oracle"]
         for a, b in zip(pl, oracle.decode(f["oracle"])):
             assert not a.is_cuda and np.array_equal(a.numpy(), b)
+
+
+@pytest.mark.parametrize("block", [4, 8, 16, 32])
+def test_wavefront_knobs_keep_the_bytes(cuda, mixed, block):
+    """Every wavefront block, and warp pairs per tile (tiles of one band or
+    of fewer than 66 columns stay on one warp), write the oracle's streams
+    and decode to the oracle's planes: the knobs change only the schedule."""
+    from fastvid_b200 import autotune
+
+    before = (autotune.wavefront_block(), autotune.tile_warps())
+    extra = [dict(planes=synth.make_frame(w, h, "gray", 10, 700 + w, sigma=(3, 1)), layout="gray", bit_depth=10,
+                  quality=90, tile=tile) for w, h, tile in ((300, 257, (128, 256)), (97, 95, (97, 40)),
+                                                             (65, 200, (65, 100)), (130, 33, (130, 33)))]
+    for f in extra:
+        f["oracle"] = oracle.encode(f["planes"], layout=f["layout"], bit_depth=f["bit_depth"], quality=f["quality"],
+                                    tile_size=f["tile"])
+    frames = mixed + extra
+    try:
+        for warps in (1, 2):
+            autotune.set_wavefront_block(block)
+            autotune.set_tile_warps(warps)
+            codec = BatchCodec(cuda, use_graphs=False)
+            streams = _encode(codec, frames)
+            planes = codec.decode(streams)
+            for f, st, pl in zip(frames, streams, planes):
+                assert bytes(st.cpu().numpy().tobytes()) == f["oracle"], (block, warps)
+                for a, b in zip(pl, oracle.decode(f["oracle"])):
+                    assert np.array_equal(a.cpu().numpy(), b), (block, warps)
+    finally:
+        autotune.set_wavefront_block(before[0])
+        autotune.set_tile_warps(before[1])
