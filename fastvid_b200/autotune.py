@@ -122,12 +122,21 @@ def set_tile_warps(warps: int) -> None:
     _native.check(_native.load().fvb_set_tile_warps(int(warps)))
 
 
+def decode_overlap() -> int:
+    return int(_native.load().fvb_get_decode_overlap())
+
+
+def set_decode_overlap(on: int) -> None:
+    _native.check(_native.load().fvb_set_decode_overlap(int(on)))
+
+
 def apply(table: dict) -> None:
-    """Set the table's launch geometry, wavefront block and warps per tile
-    (process-wide)."""
+    """Set the table's launch geometry, wavefront block, warps per tile and
+    decode overlap (process-wide)."""
     set_launch(table.get("launch", {}))
     set_wavefront_block(table.get("wavefront_block", 0))
     set_tile_warps(table.get("tile_warps", 0))
+    set_decode_overlap(table.get("decode_overlap", 1))
 
 
 def tile_for(table: dict | None, layout: str, bit_depth: int, width: int, height: int, default=(256, 128)):
@@ -181,6 +190,18 @@ def tune_wavefront_block(codec, frames, params, candidates=WAVEFRONT_BLOCKS, rep
         seen[steps] = _time_batch(codec, frames, params, reps)[0]
     best = min(seen, key=seen.get)
     set_wavefront_block(best)
+    return best, {str(k): round(v, 3) for k, v in seen.items()}
+
+
+def tune_decode_overlap(codec, frames, params, reps: int = 3) -> tuple[int, dict]:
+    """dec_other beside dec_rans (1) or after it (0), whichever is faster;
+    measured after the launch caps, which decide how the two share SMs."""
+    seen = {}
+    for on in (1, 0):
+        set_decode_overlap(on)
+        seen[on] = _time_batch(codec, frames, params, reps)[0]
+    best = min(seen, key=seen.get)
+    set_decode_overlap(best)
     return best, {str(k): round(v, 3) for k, v in seen.items()}
 
 
@@ -244,11 +265,13 @@ def main(argv=None) -> int:
     block, block_ms = tune_wavefront_block(codec, frames, params, reps=args.reps)
     warps, warps_ms = tune_tile_warps(codec, frames, params, reps=args.reps)
     launch = tune_launch(codec, frames, params, reps=args.reps)
+    overlap, overlap_ms = tune_decode_overlap(codec, frames, params, reps=args.reps)
     tuned_ms = _time_batch(codec, frames, params, args.reps)[0]
     table = {"device": torch.cuda.get_device_name(dev), "sample": f"{args.frames}-frame mix",
              "size_tolerance": args.size_tolerance, "tiles": tiles, "tile_measurements_ms_bytes": measured,
              "wavefront_block": block, "wavefront_block_ms": block_ms,
              "tile_warps": warps, "tile_warps_ms": warps_ms,
+             "decode_overlap": overlap, "decode_overlap_ms": overlap_ms,
              "launch": launch, "launch_gain": {"default_ms": round(base_ms, 3), "tuned_ms": round(tuned_ms, 3)}}
     save(table, args.out)
     print(json.dumps(table))

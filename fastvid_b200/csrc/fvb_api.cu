@@ -578,6 +578,7 @@ constexpr int kDefaultCtas[K_COUNT] = {
     /*dec_rans*/ 16, /*dec_other*/ 16};
 std::atomic<int> g_ctas[K_COUNT];
 std::atomic<int> g_wavefront_block{kDefaultWavefrontBlock};
+std::atomic<int> g_decode_overlap{1};
 std::atomic<int> g_tile_warps{kDefaultTileWarps};
 
 int ctas(int kernel) {
@@ -650,6 +651,14 @@ int fvb_set_wavefront_block(int steps) {
 }
 
 int fvb_get_wavefront_block(void) { return g_wavefront_block.load(std::memory_order_relaxed); }
+
+int fvb_set_decode_overlap(int on) {
+  if (on != 0 && on != 1) return fail(FVB_ERR_ARGUMENT, "decode overlap must be 0 or 1");
+  g_decode_overlap.store(on, std::memory_order_relaxed);
+  return FVB_OK;
+}
+
+int fvb_get_decode_overlap(void) { return g_decode_overlap.load(std::memory_order_relaxed); }
 
 int fvb_set_tile_warps(int warps) {
   if (warps == 0) warps = kDefaultTileWarps;
@@ -1178,7 +1187,7 @@ int decode_enqueue(const Totals& t, int wavefront, void* workspace, int64_t work
   }
   FVB_LAUNCHED("dec_rans_tables_kernel");
   SideStream* side = nullptr;
-  if (side_ok && t.shards >= kSideStreamShards) {
+  if (side_ok && t.shards >= kSideStreamShards && g_decode_overlap.load(std::memory_order_relaxed)) {
     rc = side_stream(&side);
     if (rc) return rc;
   }

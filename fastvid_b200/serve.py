@@ -144,10 +144,13 @@ class CodecBackend:
     def make_worker_codec(self):
         from .batch import BatchCodec
 
-        # graphs per shape bucket: a worker replays the launch sequence of
-        # every bucket it has seen (captured thread-locally, beside the
-        # other workers' launches)
-        return BatchCodec(self.device, use_graphs=True, resident_workspace=True, max_cached_shapes=32)
+        # Eager launches (one per kernel per batch, sized by the batch's
+        # shape bucket).  Workers do not capture CUDA graphs: torch's capture
+        # entry synchronizes the device and empties the allocator's cache,
+        # which is not safe beside the other workers' batches in flight; a
+        # full-size serving run that captured inside the workers hit an
+        # illegal memory access.
+        return BatchCodec(self.device, use_graphs=False, resident_workspace=True, max_cached_shapes=32)
 
     def resident_bytes(self, codec) -> int:
         return codec.workspace_bytes()

@@ -102,3 +102,17 @@ def test_tile_warps_knob_round_trip_and_rejections():
         assert autotune.tile_warps() == 2
     finally:
         autotune.set_tile_warps(before)
+
+
+def test_decode_overlap_knob_round_trip_and_rejections():
+    lib = _native.load()
+    before = autotune.decode_overlap()
+    try:
+        for on in (0, 1):
+            autotune.set_decode_overlap(on)
+            assert autotune.decode_overlap() == on
+        assert lib.fvb_set_decode_overlap(2) == -1 and "decode overlap" in _native.last_error()
+        autotune.apply({"launch": {}, "decode_overlap": 0})
+        assert autotune.decode_overlap() == 0
+    finally:
+        autotune.set_decode_overlap(before)
