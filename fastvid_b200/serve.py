@@ -155,6 +155,28 @@ class CodecBackend:
     def resident_bytes(self, codec) -> int:
         return codec.workspace_bytes()
 
+    def largest_workspace(self, max_pixels: int) -> int:
+        """Workspace bytes (bucket-rounded) of the largest batch a worker may
+        run: max_pixels luma pixels of rgb444 (three samples per pixel, the
+        most samples per pixel) in 64x64 tiles, encode or decode, whichever
+        needs more.  (Batches of smaller tiles hold more shard records and
+        rANS scratch and may still grow the workspace.)"""
+        side = 4096
+        height = max(1, -(-max_pixels // side))
+        frame = Frame()
+        ws = ctypes.c_int64()
+        _native.check(self.lib.fvb_encode_plan(side, height, 2, 16, 90, 24, 1, 64, 64, ctypes.byref(frame),
+                                               ctypes.byref(ws)))
+        arr = (Frame * 1)(frame)
+        dws = ctypes.c_int64()
+        _native.check(self.lib.fvb_batch_decode_plan(arr, 1, ctypes.byref(dws)))
+        return self._bucketed(max(ws.value, dws.value))
+
+    def presize(self, codec, nbytes: int) -> int:
+        """Allocate the worker's resident workspace up front; returns its bytes."""
+        codec._workspace(nbytes)
+        return codec.workspace_bytes()
+
     def release(self, codec):
         codec.release_workspace()
 
@@ -200,11 +222,19 @@ class Server:
                  max_batch_frames: int = 64, max_batch_pixels: int = 200_000_000, backend=None,
                  warm_bytes: int | None = None):
         """warm_bytes: device memory each worker allocates and frees once at
-        start on its own stream (default: an eighth of the budget per
-        worker, at most 2 GiB), so outputs come from the allocator's cache."""
+        start on its own stream (default: a quarter of the budget per
+        worker, at most 4 GiB), so outputs come from the allocator's cache.
+        Each worker also allocates its resident workspace for the largest
+        batch it may run (max_batch_pixels) at start when all workers' fit
+        in half the budget, so the workspace never grows mid-run."""
         self.backend = backend if backend is not None else CodecBackend(device if device is not None else "cuda")
         self.budget = int(memory_budget)
-        self.warm_bytes = (min(2 << 30, self.budget // (8 * workers)) if warm_bytes is None else int(warm_bytes))
+        self.warm_bytes = (min(4 << 30, self.budget // (4 * workers)) if warm_bytes is None else int(warm_bytes))
+        self.presize_bytes = 0
+        if hasattr(self.backend, "largest_workspace"):
+            need = self.backend.largest_workspace(max_batch_pixels)
+            if need * workers <= self.budget // 2:
+                self.presize_bytes = need
         self.max_frames = max_batch_frames
         self.max_pixels = max_batch_pixels
         self._pending: collections.deque[Request] = collections.deque()
@@ -317,6 +347,11 @@ class Server:
         if hasattr(self.backend, "warm"):
             self.backend.warm(self.warm_bytes)
         codec = self.backend.make_worker_codec()
+        if self.presize_bytes:
+            held = self.backend.presize(codec, self.presize_bytes)
+            with self._cv:
+                self._resident[w] = held
+                self.peak_charged = max(self.peak_charged, sum(self._resident) + self._inflight)
         while True:
             release = False
             with self._cv:
