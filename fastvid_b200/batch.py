@@ -165,10 +165,13 @@ class BatchCodec:
     def _enc_shape(f: Frame) -> tuple:
         return (f.layout, f.bit_depth, f.quality, f.width, f.height, f.tile_w, f.tile_h, f.fps_num, f.fps_den)
 
-    def encode(self, frames, *, layout=None, bit_depth=10, quality=90, frame_rate=(24, 1), tile_size=(256, 128)):
+    def encode(self, frames, *, layout=None, bit_depth=10, quality=90, frame_rate=(24, 1), tile_size=(256, 128),
+               arena: torch.Tensor | None = None):
         """Encode a list of frames (each a tuple of CUDA uint16 planes).
 
         Scalar arguments apply to every frame; lists give one value per frame.
+        `arena`: a device uint8 buffer the streams are written into when it
+        is large enough (the caller keeps it alive and unused meanwhile).
         Returns a list of 1-D CUDA uint8 streams (views of one arena).
         """
         frames = [tuple(f) if not isinstance(f, torch.Tensor) else (f,) for f in frames]
@@ -228,7 +231,11 @@ class BatchCodec:
                     raise RuntimeError(f"frame {i}: CUDA encoder analysis failed (status {status})")
             lengths = [length for _, length in res]
             total = sum(lengths)
-            arena = torch.empty(total, dtype=torch.uint8, device=self.device)
+            if arena is not None and arena.dtype == torch.uint8 and arena.device == self.device \
+                    and arena.numel() >= total:
+                arena = arena.narrow(0, 0, total)
+            else:
+                arena = torch.empty(total, dtype=torch.uint8, device=self.device)
             outs, off, base = [], 0, arena.data_ptr()
             for length in lengths:
                 outs.append(base + off)
@@ -247,10 +254,11 @@ class BatchCodec:
     def _dec_shape(f: Frame) -> tuple:
         return (f.layout, f.bit_depth, f.quality, f.flags, f.width, f.height, f.tile_w, f.tile_h)
 
-    def decode(self, streams, predictor="wavefront", headers=None):
+    def decode(self, streams, predictor="wavefront", headers=None, arena: torch.Tensor | None = None):
         """Decode a list of 1-D uint8 streams; returns a list of plane tuples.
         `headers`: the streams' first 32 bytes when the caller has them
-        (saves reading them back from the device)."""
+        (saves reading them back from the device).  `arena`: a device
+        uint16 buffer the planes are written into when it is large enough."""
         if predictor not in ("wavefront", "serial"):
             raise ValueError("predictor must be 'wavefront' or 'serial'")
         n = len(streams)
@@ -312,7 +320,11 @@ class BatchCodec:
             slot = self._slot(self._dec, arr, n, decode=True, wavefront=wavefront)
             bucket = ctypes.byref(slot.bucket)
             total = sum(sizes)
-            arena = torch.empty(total, dtype=torch.uint16, device=self.device)
+            if arena is not None and arena.dtype == torch.uint16 and arena.device == self.device \
+                    and arena.numel() >= total:
+                arena = arena.narrow(0, 0, total)
+            else:
+                arena = torch.empty(total, dtype=torch.uint16, device=self.device)
             # plane pointers by arithmetic (Y, then Cb, then Cr of each frame);
             # the tensor views are made while the GPU decodes
             ptrs, pitches, off, base = [], [], 0, arena.data_ptr()
@@ -519,27 +531,49 @@ class BatchCodec:
         i+ahead, the encode and decode of chunk i, and the download of chunk
         i-1's streams and planes run at once, on two copy streams beside the
         compute stream, so both directions of the host link stay busy while
-        the kernels run.  The streams stay on the device between the encode
-        and the decode.  Streams equal encode()'s and planes decode()'s.
-        Returns (streams, planes), one entry per frame."""
+        the kernels run.  Device buffers are resident: a ring of ahead+1
+        upload slots and of stream and plane arenas, kept by the codec and
+        reused chunk after chunk (events order each reuse after the work
+        that last read the slot), so the pipeline makes no allocation once
+        warm.  The streams stay on the device between the encode and the
+        decode.  Streams equal encode()'s and planes decode()'s.  Returns
+        (streams, planes), one entry per frame."""
         n = len(frames)
         if n == 0:
             return [], []
         frames = [tuple(f) if not isinstance(f, torch.Tensor) else (f,) for f in frames]
         per = {k: _per_frame(v, n, k) for k, v in params.items()}
+        bounds = list(range(0, n, chunk)) + [n]
+        nchunks = len(bounds) - 1
+        slots = min(ahead + 1, nchunks)
+        chunk_samples = [sum(p.numel() for f in frames[lo:hi] for p in f) for lo, hi in zip(bounds, bounds[1:])]
+        max_samples = max(chunk_samples)
         with torch.cuda.device(self.device):
             comp = torch.cuda.current_stream(self.device)
-            h2d, d2h = torch.cuda.Stream(self.device), torch.cuda.Stream(self.device)
+            ring = self._ring(slots, max_samples)
+            h2d, d2h = ring["h2d"], ring["d2h"]
             h2d.wait_stream(comp)
             d2h.wait_stream(comp)
-            bounds = list(range(0, n, chunk)) + [n]
-            nchunks = len(bounds) - 1
             staged: dict = {}
+            freed = [None] * slots        # event: the slot's upload buffer was last read (encode done)
+            drained = [None] * slots      # event: the slot's arenas were last read (download done)
 
             def stage(i):
                 lo, hi = bounds[i], bounds[i + 1]
+                k = i % slots
+                buf = ring["up"][k]
                 with torch.cuda.stream(h2d):
-                    dev = [tuple(p.to(self.device, non_blocking=True) for p in f) for f in frames[lo:hi]]
+                    if freed[k] is not None:
+                        h2d.wait_event(freed[k])
+                    dev, off = [], 0
+                    for f in frames[lo:hi]:
+                        planes = []
+                        for p in f:
+                            v = buf.narrow(0, off, p.numel()).view(p.shape)
+                            v.copy_(p, non_blocking=True)
+                            planes.append(v)
+                            off += p.numel()
+                        dev.append(tuple(planes))
                     ev = torch.cuda.Event()
                     ev.record(h2d)
                 staged[i] = (dev, ev)
@@ -555,30 +589,37 @@ class BatchCodec:
                 stage(i)
             for i in range(nchunks):
                 dev, ev = staged.pop(i)
+                k = i % slots
                 comp.wait_event(ev)
-                for f in dev:
-                    for p in f:
-                        p.record_stream(comp)
+                if drained[k] is not None:
+                    comp.wait_event(drained[k])
                 lo, hi = bounds[i], bounds[i + 1]
-                streams = self.encode(dev, **{k: v[lo:hi] for k, v in per.items()})
-                planes = self.decode(streams, predictor=predictor)
+                streams = self.encode(dev, arena=ring["streams"][k], **{kk: v[lo:hi] for kk, v in per.items()})
+                done_enc = torch.cuda.Event()
+                done_enc.record(comp)
+                freed[k] = done_enc
+                planes = self.decode(streams, predictor=predictor, arena=ring["planes"][k])
                 if i + ahead < nchunks:
                     stage(i + ahead)
                 done = torch.cuda.Event()
                 done.record(comp)
-                s_arena = streams[0]._base if streams[0]._base is not None else streams[0]
-                first = planes[0][0]
-                p_arena = first._base if first._base is not None else first
                 s_total = sum(int(st.numel()) for st in streams)
                 p_total = sum(p.numel() for f in planes for p in f)
+                s_src = streams[0]._base if streams[0]._base is not None else streams[0]
+                p_src = planes[0][0]._base if planes[0][0]._base is not None else planes[0][0]
                 hs, cur_s = host_slice(out_streams, cur_s, s_total, torch.uint8)
                 hp, cur_p = host_slice(out_planes, cur_p, p_total, torch.uint16)
                 with torch.cuda.stream(d2h):
                     d2h.wait_event(done)
-                    s_arena.record_stream(d2h)
-                    p_arena.record_stream(d2h)
-                    hs.copy_(s_arena.narrow(0, 0, s_total), non_blocking=True)
-                    hp.copy_(p_arena.reshape(-1).narrow(0, 0, p_total), non_blocking=True)
+                    if s_src.data_ptr() != ring["streams"][k].data_ptr():
+                        s_src.record_stream(d2h)  # an arena of its own (the ring slot was too small)
+                    if p_src.data_ptr() != ring["planes"][k].data_ptr():
+                        p_src.record_stream(d2h)
+                    hs.copy_(s_src.reshape(-1).narrow(0, 0, s_total), non_blocking=True)
+                    hp.copy_(p_src.reshape(-1).narrow(0, 0, p_total), non_blocking=True)
+                    dr = torch.cuda.Event()
+                    dr.record(d2h)
+                drained[k] = dr
                 off = 0
                 for st in streams:
                     out_s.append(hs.narrow(0, off, st.numel()))
@@ -591,7 +632,25 @@ class BatchCodec:
                         off += p.numel()
                     out_p.append(tuple(views))
             d2h.synchronize()
+            comp.wait_stream(d2h)
         return out_s, out_p
+
+    def _ring(self, slots: int, samples: int) -> dict:
+        """Resident buffers of the host round trip: `slots` upload slots and
+        plane arenas of `samples` uint16, stream arenas of 2 * `samples` +
+        64 KiB bytes (a chunk whose streams are larger -- possible only for
+        near-incompressible 16-bit content -- gets an arena of its own), and
+        the two copy streams."""
+        r = getattr(self, "_ring_bufs", None)
+        if r is None or r["slots"] < slots or r["samples"] < samples:
+            r = {"slots": slots, "samples": samples,
+                 "up": [torch.empty(samples, dtype=torch.uint16, device=self.device) for _ in range(slots)],
+                 "streams": [torch.empty(2 * samples + (64 << 10), dtype=torch.uint8, device=self.device)
+                             for _ in range(slots)],
+                 "planes": [torch.empty(samples, dtype=torch.uint16, device=self.device) for _ in range(slots)],
+                 "h2d": torch.cuda.Stream(self.device), "d2h": torch.cuda.Stream(self.device)}
+            self._ring_bufs = r
+        return r
 
 
 _default: dict = {}

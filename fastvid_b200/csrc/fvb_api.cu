@@ -579,6 +579,7 @@ constexpr int kDefaultCtas[K_COUNT] = {
 std::atomic<int> g_ctas[K_COUNT];
 std::atomic<int> g_wavefront_block{kDefaultWavefrontBlock};
 std::atomic<int> g_decode_overlap{1};
+std::atomic<int> g_rans_pipeline{0};
 std::atomic<int> g_tile_warps{kDefaultTileWarps};
 
 int ctas(int kernel) {
@@ -659,6 +660,14 @@ int fvb_set_decode_overlap(int on) {
 }
 
 int fvb_get_decode_overlap(void) { return g_decode_overlap.load(std::memory_order_relaxed); }
+
+int fvb_set_rans_pipeline(int steps) {
+  if (steps != 0 && steps != 8 && steps != 16) return fail(FVB_ERR_ARGUMENT, "rANS pipeline must be 0, 8 or 16");
+  g_rans_pipeline.store(steps, std::memory_order_relaxed);
+  return FVB_OK;
+}
+
+int fvb_get_rans_pipeline(void) { return g_rans_pipeline.load(std::memory_order_relaxed); }
 
 int fvb_set_tile_warps(int warps) {
   if (warps == 0) warps = kDefaultTileWarps;
@@ -861,8 +870,9 @@ int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, 
     FVB_LAUNCHED("enc_analyze_kernel");
     {
       LaunchScope scope_(K_ENC_RANS, stream);
-      enc_rans_kernel<<<static_cast<int>(ceil_div(nsh * 4 > 0 ? nsh * 4 : 1, 128)), 128, 0, stream>>>(
-          state, dims, pass, shards, folded, rans);
+      enc_rans_launch(g_rans_pipeline.load(std::memory_order_relaxed),
+                      static_cast<int>(ceil_div(nsh * 4 > 0 ? nsh * 4 : 1, 128)), stream, state, dims, pass, shards,
+                      folded, rans);
     }
     FVB_LAUNCHED("enc_rans_kernel");
     {

@@ -982,6 +982,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
 // shards per warp.  Lane bytes are written back to front so they end up in
 // stream order (the reference reverses them at emission, encode.cu:609).
 
+template <int PIPE>
 __global__ void __launch_bounds__(128)
 enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restrict__ dims, int pass,
                 ShardInfo* __restrict__ shards, const uint32_t* __restrict__ folded,
@@ -1022,23 +1023,74 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
     const uint32_t q = __umulhi(x, e.x) >> (e.y >> 25);
     x += (e.y & 0x1fffu) + q * cmpl;
   };
-  // symbols and table entries are loaded kAhead steps ahead of the state chain
-  constexpr int kAhead = 16;  // measured on the 96-frame mix: 16 beats 4, 8 and 32
   int c = 0;
-  for (; c + kAhead <= steps; c += kAhead) {
-    uint32_t v[kAhead];
-    uint2 e[kAhead];
+  if (PIPE == 0) {
+    // symbols and table entries are loaded 16 steps ahead of the state chain
+    constexpr int kAhead = 16;
+    for (; c + kAhead <= steps; c += kAhead) {
+      uint32_t v[kAhead];
+      uint2 e[kAhead];
 #pragma unroll
-    for (int j = 0; j < kAhead; ++j) v[j] = __ldg(f + first - 4 * (c + j));
+      for (int j = 0; j < kAhead; ++j) v[j] = __ldg(f + first - 4 * (c + j));
 #pragma unroll
-    for (int j = 0; j < kAhead; ++j) e[j] = tab[v[j]];
+      for (int j = 0; j < kAhead; ++j) e[j] = tab[v[j]];
 #pragma unroll
-    for (int j = 0; j < kAhead; ++j) step(e[j]);
+      for (int j = 0; j < kAhead; ++j) step(e[j]);
+    }
+  } else {
+    // Software pipeline over blocks of PIPE steps: while block b runs, the
+    // table entries of block b+1 (whose symbols arrived a block earlier) and
+    // the symbols of block b+2 are in flight, so neither the symbol load nor
+    // the dependent table load sits on the state chain.
+    constexpr int kB = PIPE > 0 ? PIPE : 1;
+    const int nblk = steps / kB;
+    uint32_t vn[kB];      // symbols of block b+2
+    uint2 en[kB], ec[kB];  // table entries of blocks b+1 and b
+    auto load_v = [&](int b, uint32_t (&v)[kB]) {
+#pragma unroll
+      for (int j = 0; j < kB; ++j) v[j] = __ldg(f + first - 4 * (b * kB + j));
+    };
+    if (nblk > 0) {
+      load_v(0, vn);
+#pragma unroll
+      for (int j = 0; j < kB; ++j) ec[j] = tab[vn[j]];
+    }
+    if (nblk > 1) {
+      load_v(1, vn);
+#pragma unroll
+      for (int j = 0; j < kB; ++j) en[j] = tab[vn[j]];
+    }
+    if (nblk > 2) load_v(2, vn);
+    for (int b = 0; b < nblk; ++b) {
+      uint2 cur[kB];
+#pragma unroll
+      for (int j = 0; j < kB; ++j) {
+        cur[j] = ec[j];
+        ec[j] = en[j];
+      }
+      if (b + 2 < nblk) {
+#pragma unroll
+        for (int j = 0; j < kB; ++j) en[j] = tab[vn[j]];
+      }
+      if (b + 3 < nblk) load_v(b + 3, vn);
+#pragma unroll
+      for (int j = 0; j < kB; ++j) step(cur[j]);
+    }
+    c = nblk * kB;
   }
   for (; c < steps; ++c) step(tab[__ldg(f + first - 4 * c)]);
   if (nacc) out_end[-(nwords + 1)] = static_cast<uint32_t>(acc << (8 * (4 - nacc)));  // low bytes unused
   si.rans_lane[lane] = 4 * nwords + nacc;
   si.rans_state[lane] = x;
+}
+
+// enc_rans with its loads either 16 steps ahead in one stage (PIPE 0) or
+// pipelined over blocks of 8 or 16 steps (the autotuner's knob; identical
+// bytes).
+void enc_rans_launch(int pipe, int grid, cudaStream_t stream, const FrameState* state, const BatchDims* dims,
+                     int pass, ShardInfo* shards, const uint32_t* folded, uint8_t* rans_scratch) {
+  auto k = pipe == 8 ? enc_rans_kernel<8> : pipe == 16 ? enc_rans_kernel<16> : enc_rans_kernel<0>;
+  k<<<grid, 128, 0, stream>>>(state, dims, pass, shards, folded, rans_scratch);
 }
 
 // ---------------------------------------------------------------------------

@@ -32,8 +32,10 @@ __global__ void enc_predict_wide_kernel(const FrameDesc* frames, FrameState* sta
                                         uint32_t* folded, uint16_t* recon);
 __global__ void enc_analyze_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
                                    ShardInfo* shards, const uint32_t* folded, uint8_t* rans_scratch);
-__global__ void enc_rans_kernel(const FrameState* state, const BatchDims* dims, int pass, ShardInfo* shards,
-                                const uint32_t* folded, uint8_t* rans_scratch);
+// enc_rans with one-stage loads (pipe 0) or a software pipeline over blocks
+// of `pipe` (8 or 16) steps
+void enc_rans_launch(int pipe, int grid, cudaStream_t stream, const FrameState* state, const BatchDims* dims,
+                     int pass, ShardInfo* shards, const uint32_t* folded, uint8_t* rans_scratch);
 __global__ void enc_scan_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
                                 ShardInfo* shards, uint8_t* prefix);
 __global__ void enc_emit_kernel(const FrameDesc* frames, int nframes, const ShardInfo* shards,

@@ -98,6 +98,14 @@ int fvb_get_tile_warps(void);
  * (the autotuner's knob). */
 int fvb_set_decode_overlap(int on);
 int fvb_get_decode_overlap(void);
+/* How the rANS encoder fetches ahead of its state chain (no reference
+ * counterpart, whose lanes load as they go, cuda/csrc/encode.cu:398-418): 0
+ * loads 16 symbols and then their table entries before each 16 steps; 8 or
+ * 16 runs a software pipeline over blocks of that many steps, the symbols
+ * two blocks and the table entries one block ahead.  Process-wide, read at
+ * each launch; no output depends on it (the autotuner's knob). */
+int fvb_set_rans_pipeline(int steps);
+int fvb_get_rans_pipeline(void);
 /* While profiling is on (per calling thread), every launch is bracketed by
  * CUDA events on its stream; fvb_profile_end waits for them and writes, per
  * kernel id, the summed milliseconds and the number of launches. */

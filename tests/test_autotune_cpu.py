@@ -116,3 +116,18 @@ def test_decode_overlap_knob_round_trip_and_rejections():
         assert autotune.decode_overlap() == 0
     finally:
         autotune.set_decode_overlap(before)
+
+
+def test_rans_pipeline_knob_round_trip_and_rejections():
+    lib = _native.load()
+    before = autotune.rans_pipeline()
+    try:
+        for steps in (0, 8, 16):
+            autotune.set_rans_pipeline(steps)
+            assert autotune.rans_pipeline() == steps
+        for bad in (4, 32, -1):
+            assert lib.fvb_set_rans_pipeline(bad) == -1 and "rANS pipeline" in _native.last_error()
+        autotune.apply({"launch": {}, "rans_pipeline": 8})
+        assert autotune.rans_pipeline() == 8
+    finally:
+        autotune.set_rans_pipeline(before)

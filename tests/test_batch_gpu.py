@@ -211,3 +211,18 @@ def test_wavefront_knobs_keep_the_bytes(cuda, mixed, block):
     finally:
         autotune.set_wavefront_block(before[0])
         autotune.set_tile_warps(before[1])
+
+
+@pytest.mark.parametrize("pipe", [8, 16])
+def test_rans_pipeline_keeps_the_bytes(cuda, mixed, pipe):
+    """The pipelined rANS encoder fetch writes the oracle's streams."""
+    from fastvid_b200 import autotune
+
+    before = autotune.rans_pipeline()
+    try:
+        autotune.set_rans_pipeline(pipe)
+        codec = BatchCodec(cuda, use_graphs=False)
+        for f, st in zip(mixed, _encode(codec, mixed)):
+            assert bytes(st.cpu().numpy().tobytes()) == f["oracle"], pipe
+    finally:
+        autotune.set_rans_pipeline(before)
