@@ -36,18 +36,21 @@ class Frame(ctypes.Structure):
         return other
 
 
+ABI_VERSION = 2  # FVB_ABI_VERSION of include/fastvid_b200.h (2: fvb_bucket.fold16)
+
+
 class Bucket(ctypes.Structure):
     """Mirror of ``fvb_bucket``: a capacity that a batch fits (see the header)."""
 
     _fields_ = [
         ("frames", c_i64), ("tiles", c_i64), ("shards", c_i64), ("samples", c_i64), ("prefix", c_i64),
         ("frames_p", c_i64 * 3), ("tiles_p", c_i64 * 3), ("shards_p", c_i64 * 3),
-        ("passes", c_i32), ("wide", c_i32),
+        ("passes", c_i32), ("wide", c_i32), ("fold16", c_i32), ("pad", c_i32),
     ]
 
     def key(self) -> tuple:
         return (self.frames, self.tiles, self.shards, self.samples, self.prefix, tuple(self.frames_p),
-                tuple(self.tiles_p), tuple(self.shards_p), self.passes, self.wide)
+                tuple(self.tiles_p), tuple(self.shards_p), self.passes, self.wide, self.fold16)
 
 
 # exported symbol -> (argtypes, restype)
@@ -118,6 +121,9 @@ def load():
             fn = getattr(lib, name)
             fn.argtypes = argtypes
             fn.restype = restype
+        if lib.fvb_abi_version() != ABI_VERSION:
+            raise RuntimeError(f"{LIB_PATH} has ABI version {lib.fvb_abi_version()}, expected {ABI_VERSION}: "
+                               "rebuild it (python -m fastvid_b200.build)")
         _lib = lib
     return _lib
 

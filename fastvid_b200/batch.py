@@ -519,19 +519,23 @@ class BatchCodec:
         return out
 
 
-    def encode_decode_host(self, frames, *, chunk: int = 8, ahead: int = 3, predictor: str = "wavefront",
-                           out_streams: torch.Tensor | None = None, out_planes: torch.Tensor | None = None,
-                           **params):
+    def encode_decode_host(self, frames, *, chunk: int = 32, chunk_bytes: int = 96 << 20, ahead: int = 3,
+                           predictor: str = "wavefront", out_streams: torch.Tensor | None = None,
+                           out_planes: torch.Tensor | None = None, **params):
         """Encode frames held in (preferably pinned) host memory and decode
         the streams again -- the round trip a codec evaluation makes -- with
         the streams and the decoded planes delivered in pinned host memory
         (views of `out_streams` / `out_planes` while they have room).
 
-        The frames go through in chunks of `chunk`: the upload of chunk
-        i+ahead, the encode and decode of chunk i, and the download of chunk
-        i-1's streams and planes run at once, on two copy streams beside the
-        compute stream, so both directions of the host link stay busy while
-        the kernels run.  Device buffers are resident: a ring of ahead+1
+        The frames go through in chunks of consecutive frames, each closed
+        once it holds `chunk` frames or its next frame would take it above
+        `chunk_bytes` of samples (a larger frame is a chunk of its own): the
+        upload of chunk i+ahead, the encode and decode of chunk i, and the
+        download of chunk i-1's streams and planes run at once, on two copy
+        streams beside the compute stream, so both directions of the host
+        link stay busy while the kernels run.  Chunks of similar byte size
+        keep the pipeline's fill and drain -- the first upload and the last
+        download, which nothing overlaps -- short whatever the frame mix.  Device buffers are resident: a ring of ahead+1
         upload slots and of stream and plane arenas, kept by the codec and
         reused chunk after chunk (events order each reuse after the work
         that last read the slot), so the pipeline makes no allocation once
@@ -543,7 +547,7 @@ class BatchCodec:
             return [], []
         frames = [tuple(f) if not isinstance(f, torch.Tensor) else (f,) for f in frames]
         per = {k: _per_frame(v, n, k) for k, v in params.items()}
-        bounds = list(range(0, n, chunk)) + [n]
+        bounds = _chunk_bounds([2 * sum(p.numel() for p in f) for f in frames], chunk, chunk_bytes)
         nchunks = len(bounds) - 1
         slots = min(ahead + 1, nchunks)
         chunk_samples = [sum(p.numel() for f in frames[lo:hi] for p in f) for lo, hi in zip(bounds, bounds[1:])]
@@ -651,6 +655,20 @@ class BatchCodec:
                  "h2d": torch.cuda.Stream(self.device), "d2h": torch.cuda.Stream(self.device)}
             self._ring_bufs = r
         return r
+
+
+def _chunk_bounds(sizes: list[int], max_frames: int, max_bytes: int) -> list[int]:
+    """Chunk boundaries over consecutive items: a chunk closes at
+    `max_frames` items or before the item that would take it above
+    `max_bytes` (an item larger than that is a chunk of its own)."""
+    bounds, acc = [0], 0
+    for i, b in enumerate(sizes):
+        if i > bounds[-1] and (acc + b > max_bytes or i - bounds[-1] >= max_frames):
+            bounds.append(i)
+            acc = 0
+        acc += b
+    bounds.append(len(sizes))
+    return bounds
 
 
 _default: dict = {}

@@ -274,15 +274,12 @@ int ensure_smem_attrs() {
   FVB_CUDA(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && done[dev]) return FVB_OK;
   FVB_CUDA(enc_predict_set_smem());
-  FVB_CUDA(cudaFuncSetAttribute(enc_emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(enc_emit_smem())));
+  FVB_CUDA(enc_emit_set_smem(static_cast<int>(enc_emit_smem())));
   FVB_CUDA(dec_reconstruct_set_smem());
-  FVB_CUDA(cudaFuncSetAttribute(dec_rans_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(dec_rans_smem())));
+  FVB_CUDA(dec_rans_set_attr(cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dec_rans_smem())));
   // the whole unified L1/shared array as shared memory: four dec_rans CTAs
   // (56 KB each) per SM
-  FVB_CUDA(cudaFuncSetAttribute(dec_rans_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                cudaSharedmemCarveoutMaxShared));
+  FVB_CUDA(dec_rans_set_attr(cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
   if (dev >= 0 && dev < 64) done[dev] = true;
   return FVB_OK;
 }
@@ -308,6 +305,7 @@ struct Totals {
   int frames = 0;
   int64_t tiles = 0, shards = 0, samples = 0, prefix = 0;
   bool wide = false;
+  bool fold16 = true;  // folded symbols held as u16 (every frame below depth 16 or quality 100)
   int passes = 1;
   // frames, tiles and shards that take part in pass p; the encoder lays the
   // batch out with frames of more passes first, so these are prefixes
@@ -326,6 +324,7 @@ Totals totals_of(const fvb_frame* frames, int n) {
     t.prefix += f.prefix_bytes;
     const int64_t ptw0 = f.tile_w;
     if (ptw0 > kFastMaxW) t.wide = true;
+    if (f.bit_depth >= 16 && f.quality >= 100) t.fold16 = false;
     const int passes = frame_passes(f);
     if (passes > t.passes) t.passes = passes;
     for (int p = 0; p < passes; ++p) {
@@ -364,10 +363,11 @@ BatchDims dims_of(const Totals& t) {
 }
 
 // A batch fits a capacity when every count is within it and the launch
-// sequence is the same (encoder passes, wide-tile kernels).
+// sequence is the same (encoder passes, wide-tile kernels); a u32 capacity
+// also serves a batch whose symbols would fit u16.
 bool fits(const Totals& a, const Totals& cap) {
   if (a.frames > cap.frames || a.tiles > cap.tiles || a.shards > cap.shards || a.samples > cap.samples ||
-      a.prefix > cap.prefix || a.passes != cap.passes || a.wide != cap.wide)
+      a.prefix > cap.prefix || a.passes != cap.passes || a.wide != cap.wide || (cap.fold16 && !a.fold16))
     return false;
   for (int p = 0; p < kMaxPasses; ++p)
     if (a.frames_p[p] > cap.frames_p[p] || a.tiles_p[p] > cap.tiles_p[p] || a.shards_p[p] > cap.shards_p[p])
@@ -414,6 +414,7 @@ void to_bucket(const Totals& t, fvb_bucket* b) {
   }
   b->passes = t.passes;
   b->wide = t.wide ? 1 : 0;
+  b->fold16 = t.fold16 ? 1 : 0;
 }
 
 int from_bucket(const fvb_bucket* b, Totals* t) {
@@ -435,6 +436,7 @@ int from_bucket(const fvb_bucket* b, Totals* t) {
   }
   t->passes = b->passes;
   t->wide = b->wide != 0;
+  t->fold16 = b->fold16 != 0;
   return FVB_OK;
 }
 
@@ -458,7 +460,7 @@ EncLayout enc_layout(const Totals& t) {
   w.queue = take(kAlign);
   w.results = take(16 * static_cast<size_t>(n));
   w.shards = take(sizeof(ShardInfo) * t.shards);
-  w.folded = take(4 * static_cast<size_t>(t.samples));
+  w.folded = take((t.fold16 ? 2 : 4) * static_cast<size_t>(t.samples));
   w.rans = take(static_cast<size_t>(kRansScratchBytes) * t.shards);
   w.prefix = take(static_cast<size_t>(t.prefix));
   w.recon = take(t.wide ? 2 * static_cast<size_t>(t.samples) : 0);
@@ -488,7 +490,7 @@ DecLayout dec_layout(const Totals& t) {
   w.lists = take(sizeof(DecodeLists));
   w.items = take(4 * 4 * static_cast<size_t>(t.shards));
   w.tables = take(dec_rans_table_bytes() * static_cast<size_t>(t.shards));
-  w.folded = take(4 * static_cast<size_t>(t.samples));
+  w.folded = take((t.fold16 ? 2 : 4) * static_cast<size_t>(t.samples));
   w.total = o;
   return w;
 }
@@ -830,7 +832,8 @@ int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, 
   FrameState* state = reinterpret_cast<FrameState*>(ws + L.state);
   int* queue = reinterpret_cast<int*>(ws + L.queue);
   ShardInfo* shards = reinterpret_cast<ShardInfo*>(ws + L.shards);
-  uint32_t* folded = reinterpret_cast<uint32_t*>(ws + L.folded);
+  void* folded = ws + L.folded;  // u16 or u32 symbols (cap.fold16)
+  const bool f16 = cap.fold16;
   uint8_t* rans = reinterpret_cast<uint8_t*>(ws + L.rans);
   uint8_t* prefix = reinterpret_cast<uint8_t*>(ws + L.prefix);
   uint16_t* recon = reinterpret_cast<uint16_t*>(ws + L.recon);
@@ -848,7 +851,7 @@ int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, 
     {
       LaunchScope scope_(K_ENC_PREDICT, stream);
       const int tw = g_tile_warps.load(std::memory_order_relaxed);
-      enc_predict_launch(g_wavefront_block.load(std::memory_order_relaxed), tw,
+      enc_predict_launch(g_wavefront_block.load(std::memory_order_relaxed), tw, f16,
                          grid_for(tiles * tw, kWarpsPerCta, ctas(K_ENC_PREDICT)), stream, frames_d, state, dims, pass,
                          shards, folded, queue);
     }
@@ -856,21 +859,21 @@ int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, 
     if (cap.wide) {
       {
         LaunchScope scope_(K_ENC_PREDICT_WIDE, stream);
-        enc_predict_wide_kernel<<<grid_for(tiles, 1, ctas(K_ENC_PREDICT_WIDE)), 256, 0, stream>>>(frames_d, state, dims,
-                                                                                                  pass, folded, recon);
+        enc_predict_wide_kernel<<<grid_for(tiles, 1, ctas(K_ENC_PREDICT_WIDE)), 256, 0, stream>>>(
+            frames_d, state, dims, pass, folded, recon, f16 ? 1 : 0);
       }
       FVB_LAUNCHED("enc_predict_wide_kernel");
     }
     {
       // resident CTAs only: each warp streams its shards through one ring
       LaunchScope scope_(K_ENC_ANALYZE, stream);
-      enc_analyze_kernel<<<grid_for(nsh, kWarpsPerCta, ctas(K_ENC_ANALYZE)), kWarpsPerCta * 32, 0, stream>>>(
-          frames_d, state, dims, pass, shards, folded, rans);
+      enc_analyze_launch(f16, grid_for(nsh, kWarpsPerCta, ctas(K_ENC_ANALYZE)), stream, frames_d, state, dims, pass,
+                         shards, folded, rans);
     }
     FVB_LAUNCHED("enc_analyze_kernel");
     {
       LaunchScope scope_(K_ENC_RANS, stream);
-      enc_rans_launch(g_rans_pipeline.load(std::memory_order_relaxed),
+      enc_rans_launch(g_rans_pipeline.load(std::memory_order_relaxed), f16,
                       static_cast<int>(ceil_div(nsh * 4 > 0 ? nsh * 4 : 1, 128)), stream, state, dims, pass, shards,
                       folded, rans);
     }
@@ -921,9 +924,9 @@ int encode_emit(const Totals& cap, const fvb_frame* frames, int n, void* workspa
   FVB_LAUNCHED("enc_prefix_kernel");
   {
     LaunchScope scope_(K_ENC_EMIT, stream);
-    enc_emit_kernel<<<grid_for(t.shards, kWarpsPerCta, ctas(K_ENC_EMIT)), kWarpsPerCta * 32, enc_emit_smem(), stream>>>(
-        frames_d, n, reinterpret_cast<const ShardInfo*>(ws + L.shards), t.shards,
-        reinterpret_cast<const uint32_t*>(ws + L.folded), reinterpret_cast<const uint8_t*>(ws + L.rans), outs_d);
+    enc_emit_launch(cap.fold16, grid_for(t.shards, kWarpsPerCta, ctas(K_ENC_EMIT)), enc_emit_smem(), stream, frames_d,
+                    n, reinterpret_cast<const ShardInfo*>(ws + L.shards), t.shards, ws + L.folded,
+                    reinterpret_cast<const uint8_t*>(ws + L.rans), outs_d);
   }
   FVB_LAUNCHED("enc_emit_kernel");
   return FVB_OK;
@@ -1177,7 +1180,8 @@ int decode_enqueue(const Totals& t, int wavefront, void* workspace, int64_t work
   FrameState* state = reinterpret_cast<FrameState*>(ws + L.state);
   int* queue = reinterpret_cast<int*>(ws + L.queue);
   ShardInfo* shards = reinterpret_cast<ShardInfo*>(ws + L.shards);
-  uint32_t* folded = reinterpret_cast<uint32_t*>(ws + L.folded);
+  void* folded = ws + L.folded;  // u16 or u32 symbols (t.fold16)
+  const bool f16 = t.fold16;
   DecodeLists* lists = reinterpret_cast<DecodeLists*>(ws + L.lists);
   int32_t* items = reinterpret_cast<int32_t*>(ws + L.items);
   FVB_CUDA(cudaMemsetAsync(state, 0, sizeof(FrameState) * n, stream));
@@ -1204,9 +1208,8 @@ int decode_enqueue(const Totals& t, int wavefront, void* workspace, int64_t work
   if (side) FVB_CUDA(cudaEventRecord(side->fork, stream));
   {
     LaunchScope scope_(K_DEC_RANS, stream);
-    dec_rans_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), kWarpsPerCta, ctas(K_DEC_RANS)), kWarpsPerCta * 32, dec_rans_smem(),
-                      stream>>>(
-        frames_d, state, shards, lists, items, tables, folded);
+    dec_rans_launch(f16, grid_for(ceil_div(t.shards, kGroupShards), kWarpsPerCta, ctas(K_DEC_RANS)), dec_rans_smem(),
+                    stream, frames_d, state, shards, lists, items, tables, folded);
   }
   FVB_LAUNCHED("dec_rans_kernel");
   {
@@ -1215,8 +1218,8 @@ int decode_enqueue(const Totals& t, int wavefront, void* workspace, int64_t work
     if (side) FVB_CUDA(cudaStreamWaitEvent(other, side->fork, 0));
     {
       LaunchScope scope_(K_DEC_OTHER, other);
-      dec_other_kernel<<<grid_for(ceil_div(t.shards, kGroupShards), 4, ctas(K_DEC_OTHER)), 128, 0, other>>>(
-          frames_d, state, shards, dims, lists, items, folded);
+      dec_other_launch(f16, grid_for(ceil_div(t.shards, kGroupShards), 4, ctas(K_DEC_OTHER)), other, frames_d, state,
+                       shards, dims, lists, items, folded);
     }
     const cudaError_t launched = cudaGetLastError();
     if (side) {  // joined even when the launch failed, so a stream capture is never left forked
@@ -1229,7 +1232,7 @@ int decode_enqueue(const Totals& t, int wavefront, void* workspace, int64_t work
     {
       LaunchScope scope_(K_DEC_RECON, stream);
       const int tw = g_tile_warps.load(std::memory_order_relaxed);
-      dec_reconstruct_launch(g_wavefront_block.load(std::memory_order_relaxed), tw,
+      dec_reconstruct_launch(g_wavefront_block.load(std::memory_order_relaxed), tw, f16,
                              grid_for(t.tiles * tw, kWarpsPerCta, ctas(K_DEC_RECON)), stream, frames_d, state, dims,
                              folded, queue);
     }
@@ -1237,15 +1240,16 @@ int decode_enqueue(const Totals& t, int wavefront, void* workspace, int64_t work
     if (t.wide) {
       {
         LaunchScope scope_(K_DEC_RECON_WIDE, stream);
-        dec_reconstruct_wide_kernel<<<grid_for(t.tiles, 1, ctas(K_DEC_RECON_WIDE)), 256, 0, stream>>>(frames_d, state, dims, folded);
+        dec_reconstruct_wide_kernel<<<grid_for(t.tiles, 1, ctas(K_DEC_RECON_WIDE)), 256, 0, stream>>>(
+            frames_d, state, dims, folded, f16 ? 1 : 0);
       }
       FVB_LAUNCHED("dec_reconstruct_wide_kernel");
     }
   } else {
     {
       LaunchScope scope_(K_DEC_RECON_SERIAL, stream);
-      dec_reconstruct_serial_kernel<<<static_cast<int>(ceil_div(t.tiles, 128)), 128, 0, stream>>>(frames_d, state, dims,
-                                                                                                 folded);
+      dec_reconstruct_serial_kernel<<<static_cast<int>(ceil_div(t.tiles, 128)), 128, 0, stream>>>(
+          frames_d, state, dims, folded, f16 ? 1 : 0);
     }
     FVB_LAUNCHED("dec_reconstruct_serial_kernel");
   }

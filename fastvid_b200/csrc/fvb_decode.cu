@@ -453,10 +453,10 @@ __device__ __forceinline__ void build_buckets(uint32_t* bcol, const uint32_t* fc
 // initial state x; the bucket table at a stride of 8 words,
 // the freq|cum and value words at a stride of 2^LOG_S.  Returns the bytes
 // consumed and the final state.
-template <int LOG_S>
+template <int LOG_S, typename FoldT>
 __device__ __forceinline__ void rans_decode_lane(const uint32_t* __restrict__ bcol, const uint32_t* __restrict__ fc_col,
                                                  const uint32_t* __restrict__ val_col, LaneRing& ring,
-                                                 uint32_t* __restrict__ out, int n, int my_l, uint32_t& x, int& cur) {
+                                                 FoldT* __restrict__ out, int n, int my_l, uint32_t& x, int& cur) {
   cur = 0;
   ring.ready();
   // Branch-free step: after x = freq*(x>>12) + slot - cum, x >= 2^11, so
@@ -470,7 +470,7 @@ __device__ __forceinline__ void rans_decode_lane(const uint32_t* __restrict__ bc
     // starts at offsets 1..r of the bucket survive the shift by 31 - r
     const uint32_t sym = (bw >> 16) + __popc(bw << ((slot & ((1u << kBucketShift) - 1u)) ^ 31u));
     const uint32_t fc = fc_col[sym << LOG_S];
-    out[idx] = val_col[sym << LOG_S];
+    out[idx] = static_cast<FoldT>(val_col[sym << LOG_S]);  // symbols below 511
     x = (fc >> 12) * (x >> kRansTableLog) + slot - (fc & ((1u << kRansTableLog) - 1u));
     const int nb = (x < kRansL) + (x < (kRansL >> 8));
     x = __funnelshift_l(static_cast<uint32_t>(win >> 32), x, 8 * nb);
@@ -496,11 +496,12 @@ __device__ __forceinline__ void rans_decode_lane(const uint32_t* __restrict__ bc
 // list, builds the shard's tables in its column and decodes its four lanes,
 // then claims another -- so every lane stays busy until the list is done,
 // whatever the mix of shards.
+template <typename FoldT>
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
 dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
                 const ShardInfo* __restrict__ shards, DecodeLists* __restrict__ lists,
                 const int32_t* __restrict__ list_items, const RansTable* __restrict__ tables,
-                uint32_t* __restrict__ folded) {
+                FoldT* __restrict__ folded) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   RansWarpSm& sm = reinterpret_cast<RansWarpSm*>(smem_raw)[warp];
@@ -520,7 +521,7 @@ dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
     const ShardInfo& si = shards[list_items[p]];
     const FrameDesc& f = frames[si.frame];
     const uint8_t* body = f.stream + si.offset;
-    uint32_t* out = folded + si.sample_base;
+    FoldT* out = folded + si.sample_base;
     uint32_t x = t.state[my_l];
     const int llen = t.lane_len[my_l];
     const uint8_t* lb = body + t.lane_start[my_l];
@@ -554,11 +555,12 @@ struct OtherGroupSm {
   int32_t valid;
 };
 
+template <typename FoldT>
 __global__ void __launch_bounds__(128)
 dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
                  const ShardInfo* __restrict__ shards, const BatchDims* __restrict__ dims,
                  DecodeLists* __restrict__ lists, const int32_t* __restrict__ list_items,
-                 uint32_t* __restrict__ folded) {
+                 FoldT* __restrict__ folded) {
   const int64_t total_shards = dims->shards_p[0];
   __shared__ OtherGroupSm sm_all[4];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -588,7 +590,7 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
     int fi = 0, mode = 0, n = 0;
     int64_t blen = 0;
     const uint8_t* body = nullptr;
-    uint32_t* out = nullptr;
+    FoldT* out = nullptr;
     uint32_t maxf = 0;
     if (s_mine >= 0) {
       const ShardInfo& si = shards[s_mine];
@@ -663,7 +665,7 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
                 ok = false;
                 break;
               }
-              out[idx] = static_cast<uint32_t>(v);
+              out[idx] = fold_store<FoldT>(static_cast<uint32_t>(v));
               if (win.nbits <= 32) win.refill();
             }
             if (ok) {
@@ -719,7 +721,7 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
               err = true;
               break;
             }
-            out[produced++] = value;
+            out[produced++] = fold_store<FoldT>(value);
           }
         }
         if (err || cursor != blen) set_status(&state[fi].status, 1);
@@ -736,7 +738,7 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
         const int fk = __shfl_sync(kFull, fi, 4 * k);
         const uint32_t mk = __shfl_sync(kFull, maxf, 4 * k);
         const uint8_t* bodyk = reinterpret_cast<const uint8_t*>(__shfl_sync(kFull, reinterpret_cast<uintptr_t>(body), 4 * k));
-        uint32_t* outk = reinterpret_cast<uint32_t*>(__shfl_sync(kFull, reinterpret_cast<uintptr_t>(out), 4 * k));
+        FoldT* outk = reinterpret_cast<FoldT*>(__shfl_sync(kFull, reinterpret_cast<uintptr_t>(out), 4 * k));
         const int nblk = (nk + kBlockSymbols - 1) / kBlockSymbols;
         const int maxw = 32 - __clz(mk);
         if (lane == 0) {
@@ -792,7 +794,7 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
                 v = static_cast<uint32_t>((acc >> (bit & 7)) & ((1ull << w) - 1));
               }
               if (v > mk) bad = 1;
-              outk[static_cast<int64_t>(b) * kBlockSymbols + i] = v;
+              outk[static_cast<int64_t>(b) * kBlockSymbols + i] = fold_store<FoldT>(v);
             }
           }
           if (__any_sync(kFull, bad) && lane == 0) set_status(&state[fk].status, 3);
@@ -813,19 +815,23 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
 // 64-column ring, the reconstruction goes out through another and is flushed
 // to the output plane 32 columns at a time (decode.cu:552-606).
 
+template <typename FoldT>
 struct RecWarpSmem {
-  uint32_t fold[32 * kFoldStride];  // folded-residual ring (u32, skewed)
+  static constexpr int kFS = fold_stride<FoldT>();
+  FoldT fold[32 * kFS];             // folded-residual ring (skewed)
   uint16_t out[32 * kSrcStride];    // reconstruction ring (u16, skewed)
   uint16_t carry[kFastMaxW + 128];  // row above the band, column c at index c + 32
 };
 
-size_t dec_reconstruct_smem() { return sizeof(RecWarpSmem) * kWarpsPerCta; }
+size_t dec_reconstruct_smem(bool fold16) {
+  return (fold16 ? sizeof(RecWarpSmem<uint16_t>) : sizeof(RecWarpSmem<uint32_t>)) * kWarpsPerCta;
+}
 
-template <bool MED, bool STEP1, bool EDGE, int UNROLL, bool SPLIT>
-__device__ __forceinline__ void rec_block(RecWarpSmem& sm, const uint16_t* carry_in, uint16_t* carry_out, int lane,
+template <bool MED, bool STEP1, bool EDGE, int UNROLL, bool SPLIT, typename FoldT>
+__device__ __forceinline__ void rec_block(RecWarpSmem<FoldT>& sm, const uint16_t* carry_in, uint16_t* carry_out, int lane,
                                           int t0, int W, int32_t maxs, int32_t step, bool band0, int32_t& rec,
                                           int32_t& a_prev) {
-  const uint32_t* frow = sm.fold + lane * kFoldStride + (t0 & 32);
+  const FoldT* frow = sm.fold + lane * RecWarpSmem<FoldT>::kFS + (t0 & 32);
   uint16_t* orow = sm.out + lane * kSrcStride + (t0 & 32);
   const uint16_t* crow_in = carry_in + 32 - lane + t0;  // lane 0: column t0 + u
   // one warp per tile reads and writes the same row: one pointer
@@ -858,46 +864,47 @@ __device__ __forceinline__ void rec_block(RecWarpSmem& sm, const uint16_t* carry
 // flushes the rest.  Lane 0 reads the row above the band from carry_in;
 // lane 31 writes the band's last row to carry_out (one warp per tile: the
 // same row, read before it is overwritten).
-template <bool MED, bool STEP1, int UNROLL, bool SPLIT>
+template <bool MED, bool STEP1, int UNROLL, bool SPLIT, typename FoldT>
 struct RecBand {
-  RecWarpSmem& sm;
+  static constexpr int kFS = RecWarpSmem<FoldT>::kFS;
+  RecWarpSmem<FoldT>& sm;
   int lane;
   uint16_t* __restrict__ plane;
   int64_t pitch;
   int W, H, x0, y0;
   int32_t maxs, step;
   int nchunks, nblocks;
-  const uint32_t* __restrict__ ftile;
+  const FoldT* __restrict__ ftile;
   int band_rows;
   bool band0;
   uint16_t* __restrict__ orows;
-  const uint32_t* __restrict__ frows;
+  const FoldT* __restrict__ frows;
   const uint16_t* carry_in;
   uint16_t* carry_out;
   int32_t rec, a_prev;
   uint32_t pf[32];
 
-  __device__ RecBand(const FrameDesc& f, const TileGeo& g, int32_t step_, const uint32_t* ftile_, RecWarpSmem& sm_,
-                     int lane_)
+  __device__ RecBand(const FrameDesc& f, const TileGeo& g, int32_t step_, const FoldT* ftile_,
+                     RecWarpSmem<FoldT>& sm_, int lane_)
       : sm(sm_), lane(lane_), plane(f.dst[g.plane]), pitch(f.dst_pitch[g.plane]), W(g.w), H(g.h), x0(g.x),
         y0(g.y), maxs(f.max_sample), step(step_), nchunks((g.w + 31) >> 5), nblocks((g.w + 31 + 31) >> 5),
         ftile(ftile_) {}
 
   __device__ void load_chunk(int k) {
     const int col = k * 32 + lane;
-    const uint32_t* __restrict__ p = frows + col;
+    const FoldT* __restrict__ p = frows + col;
     if (band_rows == 32 && col < W) {
 #pragma unroll
-      for (int r = 0; r < 32; ++r) pf[r] = __ldg(p + static_cast<int64_t>(r) * W);
+      for (int r = 0; r < 32; ++r) pf[r] = ldf(p + static_cast<int64_t>(r) * W);
     } else {
 #pragma unroll
-      for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && col < W) ? __ldg(p + static_cast<int64_t>(r) * W) : 0u;
+      for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && col < W) ? ldf(p + static_cast<int64_t>(r) * W) : 0u;
     }
   }
   __device__ void store_chunk(int k) {
     const int pj = k * 32 + lane;
 #pragma unroll
-    for (int r = 0; r < 32; ++r) sm.fold[r * kFoldStride + ((pj + r) & 63)] = pf[r];
+    for (int r = 0; r < 32; ++r) sm.fold[r * kFS + ((pj + r) & 63)] = static_cast<FoldT>(pf[r]);
   }
   __device__ void flush_chunk(int k) {
     const int col = k * 32 + lane;
@@ -934,9 +941,9 @@ struct RecBand {
     }
     const int t0 = blk * 32;
     if (t0 < 31 || t0 + 31 >= W)
-      rec_block<MED, STEP1, true, UNROLL, SPLIT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, band0, rec, a_prev);
+      rec_block<MED, STEP1, true, UNROLL, SPLIT, FoldT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, band0, rec, a_prev);
     else
-      rec_block<MED, STEP1, false, UNROLL, SPLIT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, band0, rec, a_prev);
+      rec_block<MED, STEP1, false, UNROLL, SPLIT, FoldT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, band0, rec, a_prev);
   }
   __device__ void end() {
     __syncwarp();
@@ -950,9 +957,9 @@ __device__ __forceinline__ void pair_sync(int pair) {
   asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");
 }
 
-template <bool MED, bool STEP1, int UNROLL, bool PAIRS>
-__device__ void rec_tile(const FrameDesc& f, const TileGeo& g, int32_t step, const uint32_t* __restrict__ ftile,
-                         RecWarpSmem* smw, int warp, int lane) {
+template <bool MED, bool STEP1, int UNROLL, bool PAIRS, typename FoldT>
+__device__ void rec_tile(const FrameDesc& f, const TileGeo& g, int32_t step, const FoldT* __restrict__ ftile,
+                         RecWarpSmem<FoldT>* smw, int warp, int lane) {
   if constexpr (PAIRS) {
     if (pair_splits(g.w, g.h)) {
       // warp pair: even bands on the first warp, odd bands on the second two
@@ -961,8 +968,8 @@ __device__ void rec_tile(const FrameDesc& f, const TileGeo& g, int32_t step, con
       // other's.  Both warps take the same number of slots (a function of the
       // tile's size only).
       const int pw = warp & 1;
-      RecWarpSmem& sm = smw[warp];
-      RecBand<MED, STEP1, UNROLL, true> rb(f, g, step, ftile, sm, lane);
+      RecWarpSmem<FoldT>& sm = smw[warp];
+      RecBand<MED, STEP1, UNROLL, true, FoldT> rb(f, g, step, ftile, sm, lane);
       const int n = rb.nblocks, nbands = (g.h + 31) >> 5;
       const int own = pw ? (nbands / 2) * n : ((nbands + 1) / 2) * n;
       const int slots = max(((nbands + 1) / 2) * n, (nbands / 2) * n + 2);
@@ -980,8 +987,8 @@ __device__ void rec_tile(const FrameDesc& f, const TileGeo& g, int32_t step, con
     }
     if (warp & 1) return;  // too small to split: the pair's first warp alone
   }
-  RecWarpSmem& sm = smw[warp];
-  RecBand<MED, STEP1, UNROLL, false> rb(f, g, step, ftile, sm, lane);
+  RecWarpSmem<FoldT>& sm = smw[warp];
+  RecBand<MED, STEP1, UNROLL, false, FoldT> rb(f, g, step, ftile, sm, lane);
   for (int band = 0; band * 32 < g.h; ++band) {
     rb.begin(band, sm.carry, sm.carry);
     for (int blk = 0; blk < rb.nblocks; ++blk) rb.block(blk);
@@ -993,10 +1000,10 @@ __device__ void rec_tile(const FrameDesc& f, const TileGeo& g, int32_t step, con
 // tile and both read it after the pair barrier (two alternating slots, so a
 // claim never overwrites a tile the other warp has yet to read); both then
 // make the same decisions from the same tile, so they meet at every barrier.
-template <int UNROLL, bool PAIRS>
+template <int UNROLL, bool PAIRS, typename FoldT>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, PAIRS ? 3 : 4)
 dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
-                       const BatchDims* __restrict__ dims, const uint32_t* __restrict__ folded,
+                       const BatchDims* __restrict__ dims, const FoldT* __restrict__ folded,
                        int* __restrict__ queue) {
   static_assert(kWarpsPerCta % 2 == 0, "warp pairs");
   constexpr bool pairs = PAIRS;
@@ -1005,7 +1012,7 @@ dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* _
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int64_t claimed[kWarpsPerCta / 2][2];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  RecWarpSmem* smw = reinterpret_cast<RecWarpSmem*>(smem_raw);
+  RecWarpSmem<FoldT>* smw = reinterpret_cast<RecWarpSmem<FoldT>*>(smem_raw);
   for (int it = 0;; ++it) {
     int64_t t = 0;
     if (pairs) {
@@ -1022,13 +1029,13 @@ dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* _
     if (state[fi].status != 0) continue;
     const TileGeo g = tile_geo(f, t - f.tile_base);
     if (g.w > kFastMaxW) continue;
-    const uint32_t* ftile = folded + f.sample_base + g.sample_base;
+    const FoldT* ftile = folded + f.sample_base + g.sample_base;
     if (f.use_med0) {
-      if (f.step0 == 1) rec_tile<true, true, UNROLL, PAIRS>(f, g, 1, ftile, smw, warp, lane);
-      else rec_tile<true, false, UNROLL, PAIRS>(f, g, f.step0, ftile, smw, warp, lane);
+      if (f.step0 == 1) rec_tile<true, true, UNROLL, PAIRS, FoldT>(f, g, 1, ftile, smw, warp, lane);
+      else rec_tile<true, false, UNROLL, PAIRS, FoldT>(f, g, f.step0, ftile, smw, warp, lane);
     } else {
-      if (f.step0 == 1) rec_tile<false, true, UNROLL, PAIRS>(f, g, 1, ftile, smw, warp, lane);
-      else rec_tile<false, false, UNROLL, PAIRS>(f, g, f.step0, ftile, smw, warp, lane);
+      if (f.step0 == 1) rec_tile<false, true, UNROLL, PAIRS, FoldT>(f, g, 1, ftile, smw, warp, lane);
+      else rec_tile<false, false, UNROLL, PAIRS, FoldT>(f, g, f.step0, ftile, smw, warp, lane);
     }
   }
 }
@@ -1036,30 +1043,76 @@ dec_reconstruct_kernel(const FrameDesc* __restrict__ frames, const FrameState* _
 // The wavefront block of dec_reconstruct is a launch-time choice, as for
 // enc_predict (4, 8, 16 or 32 steps unrolled; identical planes).
 cudaError_t dec_reconstruct_set_smem() {
-  const int bytes = static_cast<int>(dec_reconstruct_smem());
-  for (auto k : {dec_reconstruct_kernel<4, false>, dec_reconstruct_kernel<8, false>, dec_reconstruct_kernel<16, false>,
-                 dec_reconstruct_kernel<32, false>, dec_reconstruct_kernel<8, true>}) {
-    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  const int b32 = static_cast<int>(dec_reconstruct_smem(false)), b16 = static_cast<int>(dec_reconstruct_smem(true));
+  for (auto k : {dec_reconstruct_kernel<4, false, uint32_t>, dec_reconstruct_kernel<8, false, uint32_t>,
+                 dec_reconstruct_kernel<16, false, uint32_t>, dec_reconstruct_kernel<32, false, uint32_t>,
+                 dec_reconstruct_kernel<8, true, uint32_t>}) {
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b32);
+    if (e != cudaSuccess) return e;
+  }
+  for (auto k : {dec_reconstruct_kernel<4, false, uint16_t>, dec_reconstruct_kernel<8, false, uint16_t>,
+                 dec_reconstruct_kernel<16, false, uint16_t>, dec_reconstruct_kernel<32, false, uint16_t>,
+                 dec_reconstruct_kernel<8, true, uint16_t>}) {
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b16);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
 
-void dec_reconstruct_launch(int unroll, int tile_warps, int grid, cudaStream_t stream, const FrameDesc* frames,
-                            const FrameState* state, const BatchDims* dims, const uint32_t* folded, int* queue) {
+template <typename FoldT>
+static void dec_reconstruct_launch_t(int unroll, int tile_warps, int grid, cudaStream_t stream,
+                                     const FrameDesc* frames, const FrameState* state, const BatchDims* dims,
+                                     const void* folded, int* queue) {
   // warp pairs run with the default wavefront block
-  auto k = tile_warps == 2 ? dec_reconstruct_kernel<8, true>
-           : unroll == 4   ? dec_reconstruct_kernel<4, false>
-           : unroll == 16  ? dec_reconstruct_kernel<16, false>
-           : unroll == 32  ? dec_reconstruct_kernel<32, false>
-                           : dec_reconstruct_kernel<8, false>;
-  k<<<grid, kWarpsPerCta * 32, dec_reconstruct_smem(), stream>>>(frames, state, dims, folded, queue);
+  auto k = tile_warps == 2 ? dec_reconstruct_kernel<8, true, FoldT>
+           : unroll == 4   ? dec_reconstruct_kernel<4, false, FoldT>
+           : unroll == 16  ? dec_reconstruct_kernel<16, false, FoldT>
+           : unroll == 32  ? dec_reconstruct_kernel<32, false, FoldT>
+                           : dec_reconstruct_kernel<8, false, FoldT>;
+  k<<<grid, kWarpsPerCta * 32, dec_reconstruct_smem(sizeof(FoldT) == 2), stream>>>(
+      frames, state, dims, static_cast<const FoldT*>(folded), queue);
+}
+
+void dec_reconstruct_launch(int unroll, int tile_warps, bool fold16, int grid, cudaStream_t stream,
+                            const FrameDesc* frames, const FrameState* state, const BatchDims* dims,
+                            const void* folded, int* queue) {
+  if (fold16) dec_reconstruct_launch_t<uint16_t>(unroll, tile_warps, grid, stream, frames, state, dims, folded, queue);
+  else dec_reconstruct_launch_t<uint32_t>(unroll, tile_warps, grid, stream, frames, state, dims, folded, queue);
+}
+
+void dec_rans_launch(bool fold16, int grid, size_t smem, cudaStream_t stream, const FrameDesc* frames,
+                     FrameState* state, const ShardInfo* shards, DecodeLists* lists, const int32_t* list_items,
+                     const RansTable* tables, void* folded) {
+  if (fold16)
+    dec_rans_kernel<uint16_t><<<grid, kWarpsPerCta * 32, smem, stream>>>(frames, state, shards, lists, list_items,
+                                                                         tables, static_cast<uint16_t*>(folded));
+  else
+    dec_rans_kernel<uint32_t><<<grid, kWarpsPerCta * 32, smem, stream>>>(frames, state, shards, lists, list_items,
+                                                                         tables, static_cast<uint32_t*>(folded));
+}
+
+cudaError_t dec_rans_set_attr(cudaFuncAttribute attr, int value) {
+  const cudaError_t e = cudaFuncSetAttribute(dec_rans_kernel<uint16_t>, attr, value);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(dec_rans_kernel<uint32_t>, attr, value);
+}
+
+void dec_other_launch(bool fold16, int grid, cudaStream_t stream, const FrameDesc* frames, FrameState* state,
+                      const ShardInfo* shards, const BatchDims* dims, DecodeLists* lists, const int32_t* list_items,
+                      void* folded) {
+  if (fold16)
+    dec_other_kernel<uint16_t><<<grid, 128, 0, stream>>>(frames, state, shards, dims, lists, list_items,
+                                                         static_cast<uint16_t*>(folded));
+  else
+    dec_other_kernel<uint32_t><<<grid, 128, 0, stream>>>(frames, state, shards, dims, lists, list_items,
+                                                         static_cast<uint32_t*>(folded));
 }
 
 // Wide tiles: antidiagonal order with neighbours read back from the output
 // plane (decode.cu:572-605).
 __global__ void dec_reconstruct_wide_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
-                                            const BatchDims* __restrict__ dims, const uint32_t* __restrict__ folded) {
+                                            const BatchDims* __restrict__ dims, const void* __restrict__ folded,
+                                            int fold16) {
   const int nframes = dims->frames_p[0];
   const int64_t total_tiles = dims->tiles_p[0];
   for (int64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
@@ -1070,7 +1123,7 @@ __global__ void dec_reconstruct_wide_kernel(const FrameDesc* __restrict__ frames
     if (g.w <= kFastMaxW) continue;
     uint16_t* plane = f.dst[g.plane];
     const int64_t pitch = f.dst_pitch[g.plane];
-    const uint32_t* ftile = folded + f.sample_base + g.sample_base;
+    const int64_t fbase = f.sample_base + g.sample_base;
     const int32_t maxs = f.max_sample, step = f.step0;
     for (int d = 0; d < g.w + g.h - 1; ++d) {
       const int y0 = max(0, d - g.w + 1), y1 = min(d, g.h - 1);
@@ -1081,7 +1134,8 @@ __global__ void dec_reconstruct_wide_kernel(const FrameDesc* __restrict__ frames
         const int32_t a = y > 0 ? o[-pitch] : 0;
         const int32_t ul = (x > 0 && y > 0) ? o[-pitch - 1] : 0;
         const int32_t pred = f.use_med0 ? predict_med(l, a, ul) : predict_grad(l, a, ul, maxs);
-        *o = static_cast<uint16_t>(max(0, min(maxs, pred + unzigzag(ftile[static_cast<int64_t>(y) * g.w + x]) * step)));
+        const uint32_t fv = fold_at(folded, fold16, fbase + static_cast<int64_t>(y) * g.w + x);
+        *o = static_cast<uint16_t>(max(0, min(maxs, pred + unzigzag(fv) * step)));
       }
       __syncthreads();
     }
@@ -1090,7 +1144,8 @@ __global__ void dec_reconstruct_wide_kernel(const FrameDesc* __restrict__ frames
 
 // predictor="serial": one thread per tile in raster order (decode.cu:608-656).
 __global__ void dec_reconstruct_serial_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
-                                              const BatchDims* __restrict__ dims, const uint32_t* __restrict__ folded) {
+                                              const BatchDims* __restrict__ dims, const void* __restrict__ folded,
+                                              int fold16) {
   const int nframes = dims->frames_p[0];
   const int64_t total_tiles = dims->tiles_p[0];
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -1101,17 +1156,17 @@ __global__ void dec_reconstruct_serial_kernel(const FrameDesc* __restrict__ fram
   const TileGeo g = tile_geo(f, t - f.tile_base);
   uint16_t* plane = f.dst[g.plane];
   const int64_t pitch = f.dst_pitch[g.plane];
-  const uint32_t* ftile = folded + f.sample_base + g.sample_base;
+  const int64_t fbase = f.sample_base + g.sample_base;
   const int32_t maxs = f.max_sample, step = f.step0;
   const bool med = f.use_med0 != 0;
   for (int y = 0; y < g.h; ++y) {
     int32_t left = 0, ul = 0;
     uint16_t* orow = plane + static_cast<int64_t>(g.y + y) * pitch + g.x;
-    const uint32_t* frow = ftile + static_cast<int64_t>(y) * g.w;
+    const int64_t frow = fbase + static_cast<int64_t>(y) * g.w;
     for (int x = 0; x < g.w; ++x) {
       const int32_t a = y > 0 ? orow[x - pitch] : 0;
       const int32_t pred = med ? predict_med(left, a, ul) : predict_grad(left, a, ul, maxs);
-      const int32_t r = max(0, min(maxs, pred + unzigzag(frow[x]) * step));
+      const int32_t r = max(0, min(maxs, pred + unzigzag(fold_at(folded, fold16, frow + x)) * step));
       orow[x] = static_cast<uint16_t>(r);
       ul = a;
       left = r;

@@ -53,18 +53,20 @@ __device__ __forceinline__ int32_t div_step(uint32_t n, uint32_t magic) {
 // the instruction's immediate inside each unrolled 32-step block.  Blocks in
 // which every lane's column lies inside the tile run without predicates.
 
+template <typename FoldT>
 struct EncWarpSmem {
+  static constexpr int kFS = fold_stride<FoldT>();
   uint16_t src[32 * kSrcStride];    // source ring (u16, skewed)
-  uint32_t fold[32 * kFoldStride];  // folded-residual ring (u32, skewed)
+  FoldT fold[32 * kFS];             // folded-residual ring (skewed)
   uint16_t carry[kFastMaxW + 128];  // row above the band, column c at index c + 32
 };
 
-template <bool MED, bool STEP1, bool EDGE, int UNROLL, bool SPLIT>
-__device__ __forceinline__ void enc_block(EncWarpSmem& sm, const uint16_t* carry_in, uint16_t* carry_out, int lane,
+template <bool MED, bool STEP1, bool EDGE, int UNROLL, bool SPLIT, typename FoldT>
+__device__ __forceinline__ void enc_block(EncWarpSmem<FoldT>& sm, const uint16_t* carry_in, uint16_t* carry_out, int lane,
                                           int t0, int W, int32_t maxs, int32_t step, int32_t half, uint32_t magic,
                                           bool band0, int32_t& rec, int32_t& a_prev) {
   const uint16_t* srow = sm.src + lane * kSrcStride + (t0 & 32);
-  uint32_t* frow = sm.fold + lane * kFoldStride + (t0 & 32);
+  FoldT* frow = sm.fold + lane * EncWarpSmem<FoldT>::kFS + (t0 & 32);
   const uint16_t* crow_in = carry_in + 32 - lane + t0;  // lane 0: column t0 + u
   // one warp per tile reads and writes the same row: one pointer
   uint16_t* crow_out = SPLIT ? carry_out + 32 - lane + t0 : const_cast<uint16_t*>(crow_in);      // lane 31: column t0 + u - 31 (index (t - lane) + 32)
@@ -92,7 +94,7 @@ __device__ __forceinline__ void enc_block(EncWarpSmem& sm, const uint16_t* carry
     } else {
       if (lane == 31) crow_out[u] = static_cast<uint16_t>(rn);
     }
-    frow[u] = zigzag(q);
+    frow[u] = static_cast<FoldT>(zigzag(q));
     a_prev = a;
     rec = rn;
   }
@@ -103,9 +105,10 @@ __device__ __forceinline__ void enc_block(EncWarpSmem& sm, const uint16_t* carry
 // source chunks, block(k) runs wavefront block k (staging the chunk ahead
 // and flushing the folded residuals two chunks behind), end() flushes the
 // rest.  vmax tracks the largest source sample read (the depth check).
-template <bool MED, bool STEP1, int UNROLL, bool SPLIT>
+template <bool MED, bool STEP1, int UNROLL, bool SPLIT, typename FoldT>
 struct EncBand {
-  EncWarpSmem& sm;
+  static constexpr int kFS = EncWarpSmem<FoldT>::kFS;
+  EncWarpSmem<FoldT>& sm;
   int lane;
   const uint16_t* __restrict__ plane;
   int64_t pitch;
@@ -113,19 +116,19 @@ struct EncBand {
   int32_t maxs, step, half;
   uint32_t magic;
   int nchunks, nblocks;
-  uint32_t* __restrict__ ftile;
+  FoldT* __restrict__ ftile;
   uint32_t vmax = 0;
   int band_rows;
   bool band0;
   const uint16_t* __restrict__ rows;
-  uint32_t* __restrict__ frows;
+  FoldT* __restrict__ frows;
   const uint16_t* carry_in;
   uint16_t* carry_out;
   int32_t rec, a_prev;
   uint32_t pf[32];
 
-  __device__ EncBand(const FrameDesc& f, const TileGeo& g, int32_t step_, uint32_t magic_, uint32_t* ftile_,
-                     EncWarpSmem& sm_, int lane_)
+  __device__ EncBand(const FrameDesc& f, const TileGeo& g, int32_t step_, uint32_t magic_, FoldT* ftile_,
+                     EncWarpSmem<FoldT>& sm_, int lane_)
       : sm(sm_), lane(lane_), plane(f.src[g.plane]), pitch(f.src_pitch[g.plane]), W(g.w), H(g.h), x0(g.x), y0(g.y),
         maxs(f.max_sample), step(step_), half(step_ >> 1), magic(magic_), nchunks((g.w + 31) >> 5),
         nblocks((g.w + 31 + 31) >> 5), ftile(ftile_) {}
@@ -151,12 +154,12 @@ struct EncBand {
   __device__ void flush_chunk(int k) {
     const int col = k * 32 + lane;
     if (col < W) {
-      uint32_t* __restrict__ q = frows + col;
+      FoldT* __restrict__ q = frows + col;
       if (band_rows == 32) {
 #pragma unroll
-        for (int r = 0; r < 32; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFoldStride + ((col + r) & 63)];
+        for (int r = 0; r < 32; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFS + ((col + r) & 63)];
       } else {
-        for (int r = 0; r < band_rows; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFoldStride + ((col + r) & 63)];
+        for (int r = 0; r < band_rows; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFS + ((col + r) & 63)];
       }
     }
   }
@@ -183,10 +186,10 @@ struct EncBand {
     }
     const int t0 = blk * 32;
     if (t0 < 31 || t0 + 31 >= W)
-      enc_block<MED, STEP1, true, UNROLL, SPLIT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, half, magic, band0, rec,
+      enc_block<MED, STEP1, true, UNROLL, SPLIT, FoldT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, half, magic, band0, rec,
                                           a_prev);
     else
-      enc_block<MED, STEP1, false, UNROLL, SPLIT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, half, magic, band0, rec,
+      enc_block<MED, STEP1, false, UNROLL, SPLIT, FoldT>(sm, carry_in, carry_out, lane, t0, W, maxs, step, half, magic, band0, rec,
                                            a_prev);
   }
   __device__ void end() {
@@ -199,9 +202,10 @@ struct EncBand {
 // A tile by one warp: bands in order, one carry row (read by lane 0 before
 // lane 31 overwrites it).  Kept apart from EncBand: written as one loop nest
 // it needs no register spills.
-template <bool MED, bool STEP1, int UNROLL>
+template <bool MED, bool STEP1, int UNROLL, typename FoldT>
 __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step, uint32_t magic,
-                              uint32_t* __restrict__ folded_tile, EncWarpSmem& sm, int lane, int32_t& bad) {
+                              FoldT* __restrict__ folded_tile, EncWarpSmem<FoldT>& sm, int lane, int32_t& bad) {
+  constexpr int kFS = EncWarpSmem<FoldT>::kFS;
   const uint16_t* __restrict__ plane = f.src[g.plane];
   const int64_t pitch = f.src_pitch[g.plane];
   const int W = g.w, H = g.h;
@@ -213,7 +217,7 @@ __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
   for (int band = 0; band * 32 < H; ++band) {
     const int band_rows = min(32, H - band * 32);
     const uint16_t* __restrict__ rows = plane + static_cast<int64_t>(g.y + band * 32) * pitch + g.x;
-    uint32_t* __restrict__ frows = folded_tile + static_cast<int64_t>(band * 32) * W;
+    FoldT* __restrict__ frows = folded_tile + static_cast<int64_t>(band * 32) * W;
     uint32_t pf[32];
     auto load_chunk = [&](int k) {
       const int col = k * 32 + lane;
@@ -236,12 +240,12 @@ __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
     auto flush_chunk = [&](int k) {
       const int col = k * 32 + lane;
       if (col < W) {
-        uint32_t* __restrict__ q = frows + col;
+        FoldT* __restrict__ q = frows + col;
         if (band_rows == 32) {
 #pragma unroll
-          for (int r = 0; r < 32; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFoldStride + ((col + r) & 63)];
+          for (int r = 0; r < 32; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFS + ((col + r) & 63)];
         } else {
-          for (int r = 0; r < band_rows; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFoldStride + ((col + r) & 63)];
+          for (int r = 0; r < band_rows; ++r) q[static_cast<int64_t>(r) * W] = sm.fold[r * kFS + ((col + r) & 63)];
         }
       }
     };
@@ -261,10 +265,10 @@ __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
       const int t0 = blk * 32;
       const bool edge = t0 < 31 || t0 + 31 >= W;
       if (edge)
-        enc_block<MED, STEP1, true, UNROLL, false>(sm, sm.carry, sm.carry, lane, t0, W, maxs, step, half, magic, band0,
+        enc_block<MED, STEP1, true, UNROLL, false, FoldT>(sm, sm.carry, sm.carry, lane, t0, W, maxs, step, half, magic, band0,
                                                    rec, a_prev);
       else
-        enc_block<MED, STEP1, false, UNROLL, false>(sm, sm.carry, sm.carry, lane, t0, W, maxs, step, half, magic,
+        enc_block<MED, STEP1, false, UNROLL, false, FoldT>(sm, sm.carry, sm.carry, lane, t0, W, maxs, step, half, magic,
                                                     band0, rec, a_prev);
     }
     __syncwarp();
@@ -279,17 +283,18 @@ __device__ __forceinline__ void enc_pair_sync(int pair) {
   asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");
 }
 
-template <bool MED, bool STEP1, int UNROLL, bool PAIRS>
+template <bool MED, bool STEP1, int UNROLL, bool PAIRS, typename FoldT>
 __device__ void enc_tile(const FrameDesc& f, const TileGeo& g, int32_t step, uint32_t magic,
-                         uint32_t* __restrict__ folded_tile, EncWarpSmem* smw, int warp, int lane, int32_t& bad) {
+                         FoldT* __restrict__ folded_tile, EncWarpSmem<FoldT>* smw, int warp, int lane,
+                         int32_t& bad) {
   if constexpr (PAIRS) {
     if (pair_splits(g.w, g.h)) {
       // warp pair: even bands on the first warp, odd bands on the second two
       // blocks behind, in lock-step at the pair barrier after every slot (the
       // schedule of dec_reconstruct)
       const int pw = warp & 1;
-      EncWarpSmem& sm = smw[warp];
-      EncBand<MED, STEP1, UNROLL, true> eb(f, g, step, magic, folded_tile, sm, lane);
+      EncWarpSmem<FoldT>& sm = smw[warp];
+      EncBand<MED, STEP1, UNROLL, true, FoldT> eb(f, g, step, magic, folded_tile, sm, lane);
       const int n = eb.nblocks, nbands = (g.h + 31) >> 5;
       const int own = pw ? (nbands / 2) * n : ((nbands + 1) / 2) * n;
       const int slots = max(((nbands + 1) / 2) * n, (nbands / 2) * n + 2);
@@ -308,17 +313,17 @@ __device__ void enc_tile(const FrameDesc& f, const TileGeo& g, int32_t step, uin
     }
     if (warp & 1) return;  // too small to split: the pair's first warp alone
   }
-  enc_tile_fast<MED, STEP1, UNROLL>(f, g, step, magic, folded_tile, smw[warp], lane, bad);
+  enc_tile_fast<MED, STEP1, UNROLL, FoldT>(f, g, step, magic, folded_tile, smw[warp], lane, bad);
 }
 
 // Tiles come from a queue; with warp pairs the pair's first warp claims a
 // tile and both read it after the pair barrier (two alternating slots), and
 // both make the same decisions from it, so they meet at every barrier.
-template <int UNROLL, bool PAIRS>
+template <int UNROLL, bool PAIRS, typename FoldT>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, PAIRS ? 3 : 4)
 enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
                    const BatchDims* __restrict__ dims, int pass, ShardInfo* __restrict__ shards,
-                   uint32_t* __restrict__ folded, int* __restrict__ queue) {
+                   FoldT* __restrict__ folded, int* __restrict__ queue) {
   static_assert(kWarpsPerCta % 2 == 0, "warp pairs");
   constexpr bool pairs = PAIRS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -326,7 +331,7 @@ enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
   const int nframes = dims->frames_p[pass];
   const int64_t total_tiles = dims->tiles_p[pass];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  EncWarpSmem* smw = reinterpret_cast<EncWarpSmem*>(smem_raw);
+  EncWarpSmem<FoldT>* smw = reinterpret_cast<EncWarpSmem<FoldT>*>(smem_raw);
   for (int it = 0;; ++it) {
     int64_t t = 0;
     if (pairs) {
@@ -357,15 +362,15 @@ enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     if (g.w > kFastMaxW) continue;  // wide tiles go through enc_predict_wide_kernel
     const int32_t step = st.step;
     const uint32_t magic = step > 1 ? static_cast<uint32_t>((0x100000000ull + step - 1) / step) : 0u;
-    uint32_t* ftile = folded + f.sample_base + g.sample_base;
+    FoldT* ftile = folded + f.sample_base + g.sample_base;
     int32_t bad = 0;
     const bool med = st.use_med != 0;
     if (med) {
-      if (step == 1) enc_tile<true, true, UNROLL, PAIRS>(f, g, step, magic, ftile, smw, warp, lane, bad);
-      else enc_tile<true, false, UNROLL, PAIRS>(f, g, step, magic, ftile, smw, warp, lane, bad);
+      if (step == 1) enc_tile<true, true, UNROLL, PAIRS, FoldT>(f, g, step, magic, ftile, smw, warp, lane, bad);
+      else enc_tile<true, false, UNROLL, PAIRS, FoldT>(f, g, step, magic, ftile, smw, warp, lane, bad);
     } else {
-      if (step == 1) enc_tile<false, true, UNROLL, PAIRS>(f, g, step, magic, ftile, smw, warp, lane, bad);
-      else enc_tile<false, false, UNROLL, PAIRS>(f, g, step, magic, ftile, smw, warp, lane, bad);
+      if (step == 1) enc_tile<false, true, UNROLL, PAIRS, FoldT>(f, g, step, magic, ftile, smw, warp, lane, bad);
+      else enc_tile<false, false, UNROLL, PAIRS, FoldT>(f, g, step, magic, ftile, smw, warp, lane, bad);
     }
     if (__any_sync(kFull, bad) && lane == 0) set_status(&st.status, 1);
   }
@@ -375,33 +380,51 @@ enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
 // -- is a launch-time choice (4, 8, 16 or 32; the autotuner's knob): every
 // choice computes the same bytes.
 cudaError_t enc_predict_set_smem() {
-  const int bytes = static_cast<int>(enc_predict_smem());
-  for (auto k : {enc_predict_kernel<4, false>, enc_predict_kernel<8, false>, enc_predict_kernel<16, false>,
-                 enc_predict_kernel<32, false>, enc_predict_kernel<8, true>}) {
-    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  const int b32 = static_cast<int>(enc_predict_smem(false)), b16 = static_cast<int>(enc_predict_smem(true));
+  for (auto k : {enc_predict_kernel<4, false, uint32_t>, enc_predict_kernel<8, false, uint32_t>,
+                 enc_predict_kernel<16, false, uint32_t>, enc_predict_kernel<32, false, uint32_t>,
+                 enc_predict_kernel<8, true, uint32_t>}) {
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b32);
+    if (e != cudaSuccess) return e;
+  }
+  for (auto k : {enc_predict_kernel<4, false, uint16_t>, enc_predict_kernel<8, false, uint16_t>,
+                 enc_predict_kernel<16, false, uint16_t>, enc_predict_kernel<32, false, uint16_t>,
+                 enc_predict_kernel<8, true, uint16_t>}) {
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b16);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
 
-void enc_predict_launch(int unroll, int tile_warps, int grid, cudaStream_t stream, const FrameDesc* frames,
-                        FrameState* state, const BatchDims* dims, int pass, ShardInfo* shards, uint32_t* folded,
-                        int* queue) {
+template <typename FoldT>
+void enc_predict_launch_t(int unroll, int tile_warps, int grid, cudaStream_t stream, const FrameDesc* frames,
+                          FrameState* state, const BatchDims* dims, int pass, ShardInfo* shards, void* folded,
+                          int* queue) {
   // warp pairs run with the default wavefront block
-  auto k = tile_warps == 2 ? enc_predict_kernel<8, true>
-           : unroll == 4   ? enc_predict_kernel<4, false>
-           : unroll == 16  ? enc_predict_kernel<16, false>
-           : unroll == 32  ? enc_predict_kernel<32, false>
-                           : enc_predict_kernel<8, false>;
-  k<<<grid, kWarpsPerCta * 32, enc_predict_smem(), stream>>>(frames, state, dims, pass, shards, folded, queue);
+  auto k = tile_warps == 2 ? enc_predict_kernel<8, true, FoldT>
+           : unroll == 4   ? enc_predict_kernel<4, false, FoldT>
+           : unroll == 16  ? enc_predict_kernel<16, false, FoldT>
+           : unroll == 32  ? enc_predict_kernel<32, false, FoldT>
+                           : enc_predict_kernel<8, false, FoldT>;
+  k<<<grid, kWarpsPerCta * 32, enc_predict_smem(sizeof(FoldT) == 2), stream>>>(
+      frames, state, dims, pass, shards, static_cast<FoldT*>(folded), queue);
+}
+
+void enc_predict_launch(int unroll, int tile_warps, bool fold16, int grid, cudaStream_t stream,
+                        const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
+                        ShardInfo* shards, void* folded, int* queue) {
+  if (fold16)
+    enc_predict_launch_t<uint16_t>(unroll, tile_warps, grid, stream, frames, state, dims, pass, shards, folded, queue);
+  else
+    enc_predict_launch_t<uint32_t>(unroll, tile_warps, grid, stream, frames, state, dims, pass, shards, folded, queue);
 }
 
 // Tiles wider than kFastMaxW: one CTA per tile walks the antidiagonals with
 // the reconstruction kept in global scratch (same order as the reference,
 // encode.cu:150-192).  Only used for unusually wide tile sizes.
 __global__ void enc_predict_wide_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
-                                        const BatchDims* __restrict__ dims, int pass, uint32_t* __restrict__ folded,
-                                        uint16_t* __restrict__ recon) {
+                                        const BatchDims* __restrict__ dims, int pass, void* __restrict__ folded_raw,
+                                        uint16_t* __restrict__ recon, int fold16) {
   const int nframes = dims->frames_p[pass];
   const int64_t total_tiles = dims->tiles_p[pass];
   for (int64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
@@ -416,7 +439,7 @@ __global__ void enc_predict_wide_kernel(const FrameDesc* __restrict__ frames, Fr
     const uint16_t* plane = f.src[g.plane];
     const int64_t pitch = f.src_pitch[g.plane];
     uint16_t* rtile = recon + f.sample_base + g.sample_base;  // tile-raster scratch
-    uint32_t* ftile = folded + f.sample_base + g.sample_base;
+    const int64_t fbase = f.sample_base + g.sample_base;
     int bad = 0;
     for (int d = 0; d < g.w + g.h - 1; ++d) {
       const int y0 = max(0, d - g.w + 1), y1 = min(d, g.h - 1);
@@ -433,7 +456,8 @@ __global__ void enc_predict_wide_kernel(const FrameDesc* __restrict__ frames, Fr
         const int32_t mag = (abs(res) + step / 2) / step;
         const int32_t q = res < 0 ? -mag : mag;
         rtile[i] = static_cast<uint16_t>(max(0, min(maxs, pred + q * step)));
-        ftile[i] = zigzag(q);
+        if (fold16) static_cast<uint16_t*>(folded_raw)[fbase + i] = static_cast<uint16_t>(zigzag(q));
+        else static_cast<uint32_t*>(folded_raw)[fbase + i] = zigzag(q);
       }
       __syncthreads();
     }
@@ -523,10 +547,14 @@ __device__ __forceinline__ void run_block(RunStats& r, uint32_t zm, int32_t p0, 
   }
 }
 
+template <typename FoldT>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 6)
 enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ state,
                    const BatchDims* __restrict__ dims, int pass, ShardInfo* __restrict__ shards,
-                   const uint32_t* __restrict__ folded, uint8_t* __restrict__ rans_scratch) {
+                   const FoldT* __restrict__ folded, uint8_t* __restrict__ rans_scratch) {
+  // a lane's four symbols of a pack block: one 16-byte piece (u32 symbols)
+  // or one 8-byte piece (u16 symbols)
+  using Piece = FoldPiece<FoldT>;
   const int nframes = dims->frames_p[pass];
   const int64_t total_shards = dims->shards_p[pass];
   // Class counts: two classes share a 32-bit word (16-bit counts: a class
@@ -537,11 +565,11 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
   constexpr int kRing = 6;  // measured on the 96-frame mix: 6 pieces ahead beats 8
   __shared__ __align__(16) uint32_t hcls_all[kWarpsPerCta][2][520];
   __shared__ uint32_t list_all[kWarpsPerCta][512];
-  __shared__ __align__(16) uint4 ring_all[kWarpsPerCta][kRing * 32];
+  __shared__ __align__(16) Piece ring_all[kWarpsPerCta][kRing * 32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t (*hcls)[520] = hcls_all[warp];
   uint32_t* list = list_all[warp];
-  uint4* ring = ring_all[warp];
+  Piece* ring = ring_all[warp];
   const uint32_t lanes_below = (1u << lane) - 1u;
   for (int i = lane; i < 2 * 520 / 4; i += 32) reinterpret_cast<uint4*>(hcls[0])[i] = make_uint4(0, 0, 0, 0);
   __syncwarp();
@@ -561,11 +589,13 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
   };
   const int64_t warps_total = static_cast<int64_t>(gridDim.x) * kWarpsPerCta;
   const int64_t s0 = static_cast<int64_t>(blockIdx.x) * kWarpsPerCta + warp;
-  // Whole blocks of a shard that starts 16-byte aligned are read through the
+  // Whole blocks of a shard that starts piece-aligned are read through the
   // ring; the ragged last block and unaligned shards use direct loads.
   // Shards of frames that sit this pass out are skipped by both sides.
   auto whole_blocks = [&](int32_t count, int64_t base, int32_t frame) {
-    return streamed(frame) && (reinterpret_cast<uintptr_t>(folded + base) & 15u) == 0 ? count / kBlockSymbols : 0;
+    return streamed(frame) && (reinterpret_cast<uintptr_t>(folded + base) & (sizeof(Piece) - 1)) == 0
+               ? count / kBlockSymbols
+               : 0;
   };
   // Producer: the warp's whole blocks in shard order, kRing pieces ahead of
   // the consumer and across shard boundaries, one commit group per piece
@@ -573,13 +603,13 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
   // complete once at most kRing - 1 newer groups are pending.
   int64_t pt = s0;      // shard being fetched
   int pc = 0, pnf = 0;  // next block and whole blocks of pt
-  const uint4* pp = nullptr;
+  const Piece* pp = nullptr;
   int32_t q_count = 0, q_frame = 0;  // shard pt + warps_total, loaded one shard early
   int64_t q_base = 0;
   int pslot = 0;
   if (pt < total_shards) {
     pnf = whole_blocks(shards[pt].count, shards[pt].sample_base, shards[pt].frame);
-    pp = reinterpret_cast<const uint4*>(folded + shards[pt].sample_base);
+    pp = reinterpret_cast<const Piece*>(folded + shards[pt].sample_base);
     if (pt + warps_total < total_shards) {
       q_count = shards[pt + warps_total].count;
       q_frame = shards[pt + warps_total].frame;
@@ -592,7 +622,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
       pc = 0;
       if (pt < total_shards) {
         pnf = whole_blocks(q_count, q_base, q_frame);
-        pp = reinterpret_cast<const uint4*>(folded + q_base);
+        pp = reinterpret_cast<const Piece*>(folded + q_base);
         if (pt + warps_total < total_shards) {
           q_count = shards[pt + warps_total].count;
           q_frame = shards[pt + warps_total].frame;
@@ -601,7 +631,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
       }
     }
     if (pt < total_shards) {
-      cp_async16(ring + pslot * 32 + lane, pp + pc * 32 + lane);
+      cp_async_piece(ring + pslot * 32 + lane, pp + pc * 32 + lane);
       ++pc;
     }
     cp_async_commit();
@@ -630,7 +660,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     if (!streamed(frame)) continue;
     FrameState& st = state[frame];
     const int32_t active = st.active;  // first needed after pass 1
-    const uint32_t* __restrict__ f = folded + base;
+    const FoldT* __restrict__ f = folded + base;
     const int lane_count = min(4, n);
 
     // ---- pass 1 ----
@@ -660,8 +690,8 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
       const int ge = min(g + 8, nfull);
       for (int b = g; b < ge; ++b) {
         cp_async_wait<kRing - 1>();
-        const uint4 q = ring[cslot * 32 + lane];
-        const uint32_t x[4] = {q.x, q.y, q.z, q.w};
+        uint32_t x[4];
+        unpack_piece(ring[cslot * 32 + lane], x);
 #pragma unroll
         for (int j = 0; j < 4; ++j) nib[j] += bit_or_zero(x[j] << 2);  // values >= 8 add nothing
         const uint32_t bm = __reduce_max_sync(kFull, max(max(x[0], x[1]), max(x[2], x[3])));
@@ -681,7 +711,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const bool ok = p0 + j < n;
-        x[j] = ok ? __ldg(f + p0 + j) : 0u;
+        x[j] = ok ? ldf(f + p0 + j) : 0u;
         valid |= ok ? 1u << j : 0u;
         nib[j] += ok ? bit_or_zero(x[j] << 2) : 0u;
       }
@@ -787,7 +817,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
       const int nchunk = (n + 31) >> 5;
       for (int m = 0; m < nchunk; ++m) {
         const int idx = m * 32 + lane;
-        const uint32_t v = idx < n ? __ldg(f + idx) : 0u;
+        const uint32_t v = idx < n ? ldf(f + idx) : 0u;
         const int kb = bitlen(__reduce_max_sync(kFull, v));
 #pragma unroll
         for (int k = 0; k < 4; ++k) sk[k] += v >> k;
@@ -982,10 +1012,10 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
 // shards per warp.  Lane bytes are written back to front so they end up in
 // stream order (the reference reverses them at emission, encode.cu:609).
 
-template <int PIPE>
+template <int PIPE, typename FoldT>
 __global__ void __launch_bounds__(128)
 enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restrict__ dims, int pass,
-                ShardInfo* __restrict__ shards, const uint32_t* __restrict__ folded,
+                ShardInfo* __restrict__ shards, const FoldT* __restrict__ folded,
                 uint8_t* __restrict__ rans_scratch) {
   const int64_t total_shards = dims->shards_p[pass];
   const int64_t gid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -995,7 +1025,7 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
   ShardInfo& si = shards[s];
   if (!state[si.frame].active || !si.rans_ok) return;
   const int n = si.count;
-  const uint32_t* __restrict__ f = folded + si.sample_base;
+  const FoldT* __restrict__ f = folded + si.sample_base;
   uint8_t* base = rans_scratch + s * static_cast<int64_t>(kRansScratchBytes);
   const uint2* __restrict__ tab = reinterpret_cast<const uint2*>(base);
   uint32_t* out_end = reinterpret_cast<uint32_t*>(base + kRansTableWords * 4 + kRansSerialBytes +
@@ -1031,7 +1061,7 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
       uint32_t v[kAhead];
       uint2 e[kAhead];
 #pragma unroll
-      for (int j = 0; j < kAhead; ++j) v[j] = __ldg(f + first - 4 * (c + j));
+      for (int j = 0; j < kAhead; ++j) v[j] = ldf(f + first - 4 * (c + j));
 #pragma unroll
       for (int j = 0; j < kAhead; ++j) e[j] = tab[v[j]];
 #pragma unroll
@@ -1048,7 +1078,7 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
     uint2 en[kB], ec[kB];  // table entries of blocks b+1 and b
     auto load_v = [&](int b, uint32_t (&v)[kB]) {
 #pragma unroll
-      for (int j = 0; j < kB; ++j) v[j] = __ldg(f + first - 4 * (b * kB + j));
+      for (int j = 0; j < kB; ++j) v[j] = ldf(f + first - 4 * (b * kB + j));
     };
     if (nblk > 0) {
       load_v(0, vn);
@@ -1078,7 +1108,7 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
     }
     c = nblk * kB;
   }
-  for (; c < steps; ++c) step(tab[__ldg(f + first - 4 * c)]);
+  for (; c < steps; ++c) step(tab[ldf(f + first - 4 * c)]);
   if (nacc) out_end[-(nwords + 1)] = static_cast<uint32_t>(acc << (8 * (4 - nacc)));  // low bytes unused
   si.rans_lane[lane] = 4 * nwords + nacc;
   si.rans_state[lane] = x;
@@ -1087,10 +1117,31 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
 // enc_rans with its loads either 16 steps ahead in one stage (PIPE 0) or
 // pipelined over blocks of 8 or 16 steps (the autotuner's knob; identical
 // bytes).
-void enc_rans_launch(int pipe, int grid, cudaStream_t stream, const FrameState* state, const BatchDims* dims,
-                     int pass, ShardInfo* shards, const uint32_t* folded, uint8_t* rans_scratch) {
-  auto k = pipe == 8 ? enc_rans_kernel<8> : pipe == 16 ? enc_rans_kernel<16> : enc_rans_kernel<0>;
-  k<<<grid, 128, 0, stream>>>(state, dims, pass, shards, folded, rans_scratch);
+template <typename FoldT>
+static void enc_rans_launch_t(int pipe, int grid, cudaStream_t stream, const FrameState* state,
+                              const BatchDims* dims, int pass, ShardInfo* shards, const void* folded,
+                              uint8_t* rans_scratch) {
+  auto k = pipe == 8    ? enc_rans_kernel<8, FoldT>
+           : pipe == 16 ? enc_rans_kernel<16, FoldT>
+                        : enc_rans_kernel<0, FoldT>;
+  k<<<grid, 128, 0, stream>>>(state, dims, pass, shards, static_cast<const FoldT*>(folded), rans_scratch);
+}
+
+void enc_rans_launch(int pipe, bool fold16, int grid, cudaStream_t stream, const FrameState* state,
+                     const BatchDims* dims, int pass, ShardInfo* shards, const void* folded, uint8_t* rans_scratch) {
+  if (fold16) enc_rans_launch_t<uint16_t>(pipe, grid, stream, state, dims, pass, shards, folded, rans_scratch);
+  else enc_rans_launch_t<uint32_t>(pipe, grid, stream, state, dims, pass, shards, folded, rans_scratch);
+}
+
+void enc_analyze_launch(bool fold16, int grid, cudaStream_t stream, const FrameDesc* frames, FrameState* state,
+                        const BatchDims* dims, int pass, ShardInfo* shards, const void* folded,
+                        uint8_t* rans_scratch) {
+  if (fold16)
+    enc_analyze_kernel<uint16_t><<<grid, kWarpsPerCta * 32, 0, stream>>>(
+        frames, state, dims, pass, shards, static_cast<const uint16_t*>(folded), rans_scratch);
+  else
+    enc_analyze_kernel<uint32_t><<<grid, kWarpsPerCta * 32, 0, stream>>>(
+        frames, state, dims, pass, shards, static_cast<const uint32_t*>(folded), rans_scratch);
 }
 
 // ---------------------------------------------------------------------------
@@ -1290,7 +1341,9 @@ struct EmitWarpSmem {
 };
 static_assert(sizeof(EmitWarpSmem) % 16 == 0, "record buffers must stay 16-byte aligned");
 
-size_t enc_predict_smem() { return sizeof(EncWarpSmem) * kWarpsPerCta; }
+size_t enc_predict_smem(bool fold16) {
+  return (fold16 ? sizeof(EncWarpSmem<uint16_t>) : sizeof(EncWarpSmem<uint32_t>)) * kWarpsPerCta;
+}
 size_t enc_emit_smem() { return sizeof(EmitWarpSmem) * kWarpsPerCta; }
 
 // Every write into the record buffer is bounds-checked: a record can never
@@ -1369,9 +1422,10 @@ __device__ __forceinline__ void put_words(uint32_t* buf, int pos, uint32_t v, in
   if (sh && w + 1 < kEmitWords) atomicOr(&buf[w + 1], v >> (32 - sh));
 }
 
+template <typename FoldT>
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
 enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardInfo* __restrict__ shards,
-                int64_t total_shards, const uint32_t* __restrict__ folded,
+                int64_t total_shards, const FoldT* __restrict__ folded,
                 const uint8_t* __restrict__ rans_scratch, uint8_t* const* __restrict__ outs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1386,7 +1440,7 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
     for (int i = lane; 4 * i <= nwords; i += 32) reinterpret_cast<uint4*>(buf)[i] = make_uint4(0, 0, 0, 0);
     __syncwarp();
     if (lane == 0) atomicOr(&buf[0], static_cast<uint32_t>(mode) | (static_cast<uint32_t>(body & 0xffff) << 8));
-    const uint32_t* __restrict__ f = folded + si.sample_base;
+    const FoldT* __restrict__ f = folded + si.sample_base;
     if (mode == kModeZeroRun) {
       // Tokens in symbol order (encode.cu:514-536): a zero run of length L is
       // varint(2(L-1)), a value v is varint(2v-1).  A run's token is written
@@ -1394,12 +1448,12 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
       int cursor = 3;
       int run_start = 0;  // first index of the zero run reaching the chunk start
       const int nchunk = (n + 31) >> 5;
-      uint32_t v_next = lane < n ? __ldg(f + lane) : 1u;  // loaded one chunk ahead
+      uint32_t v_next = lane < n ? ldf(f + lane) : 1u;  // loaded one chunk ahead
       for (int m = 0; m < nchunk; ++m) {
         const int idx = m * 32 + lane;
         const bool valid = idx < n;
         const uint32_t v = v_next;  // past the end acts as a terminator
-        v_next = idx + 32 < n ? __ldg(f + idx + 32) : 1u;
+        v_next = idx + 32 < n ? ldf(f + idx + 32) : 1u;
         const uint32_t nzm = __ballot_sync(kFull, v != 0);
         const uint32_t below = nzm & ((1u << lane) - 1u);
         const int start = below ? m * 32 + (31 - __clz(below)) + 1 : run_start;
@@ -1465,7 +1519,7 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           const int idx = m * 128 + 4 * lane + c;
-          nx[c] = idx < n ? __ldg(f + idx) : 0u;
+          nx[c] = idx < n ? ldf(f + idx) : 0u;
         }
       };
       load(0);
@@ -1499,7 +1553,7 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
 #pragma unroll
           for (int i = 0; i < kBlockSymbols; i += 32) {
             const int idx = (b0 + u) * kBlockSymbols + i + lane;
-            if (idx < n) mx[u] = max(mx[u], __ldg(f + idx));
+            if (idx < n) mx[u] = max(mx[u], ldf(f + idx));
           }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -1524,7 +1578,7 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
         const int nb = min(kBlockSymbols, n - b * kBlockSymbols);
         if (w == 0) continue;
         for (int i = lane; i < nb; i += 32) {
-          const uint32_t v = f[b * kBlockSymbols + i];
+          const uint32_t v = f[b * kBlockSymbols + i];  // FoldT widened
           or_bits(buf, static_cast<int64_t>(off + 1) * 8 + static_cast<int64_t>(i) * w, v, w);
         }
       }
@@ -1584,4 +1638,23 @@ __global__ void enc_prefix_kernel(const FrameDesc* __restrict__ frames, int nfra
     dst[i] = src[i];
 }
 
+}  // namespace fvb
+
+namespace fvb {
+void enc_emit_launch(bool fold16, int grid, size_t smem, cudaStream_t stream, const FrameDesc* frames, int nframes,
+                     const ShardInfo* shards, int64_t total_shards, const void* folded, const uint8_t* rans_scratch,
+                     uint8_t* const* outs) {
+  if (fold16)
+    enc_emit_kernel<uint16_t><<<grid, kWarpsPerCta * 32, smem, stream>>>(
+        frames, nframes, shards, total_shards, static_cast<const uint16_t*>(folded), rans_scratch, outs);
+  else
+    enc_emit_kernel<uint32_t><<<grid, kWarpsPerCta * 32, smem, stream>>>(
+        frames, nframes, shards, total_shards, static_cast<const uint32_t*>(folded), rans_scratch, outs);
+}
+
+cudaError_t enc_emit_set_smem(int bytes) {
+  cudaError_t e = cudaFuncSetAttribute(enc_emit_kernel<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(enc_emit_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
 }  // namespace fvb

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define FVB_ABI_VERSION 1
+#define FVB_ABI_VERSION 2
 
 enum {
   FVB_OK = 0,
@@ -215,6 +215,7 @@ typedef struct fvb_bucket {
   int64_t frames, tiles, shards, samples, prefix;
   int64_t frames_p[3], tiles_p[3], shards_p[3]; /* per encoder pass */
   int32_t passes, wide;
+  int32_t fold16, pad; /* 1: folded symbols held as u16 (every frame below depth 16 or quality 100) */
 } fvb_bucket;
 
 /* The bucket of a batch. */
@@ -246,8 +247,8 @@ int fvb_bucket_decode_enqueue(const fvb_bucket* bucket, int wavefront, void* wor
  * and cudaFree can block and synchronise the device), components held to a
  * device-memory budget enforced elsewhere.  Same contract as fvb_decode, but
  * the scratch is a fixed 32 MiB array inside the library
- * (fvb_decode_noalloc_capacity() bytes, frames up to about 7 million samples;
- * larger frames return FVB_ERR_WORKSPACE), so no workspace is passed and
+ * (fvb_decode_noalloc_capacity() bytes, frames up to about 13 million samples,
+ * 7 million for lossless 16-bit frames; larger frames return FVB_ERR_WORKSPACE), so no workspace is passed and
  * nothing is allocated: no device memory, no streams, no events (dec_other
  * runs on the caller's stream).  Every GPU that loads the library holds the
  * array until the process exits.  The first call on a device does the

@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
     for name in names:
         assert hasattr(lib, name), name
         assert name in _native.SIGNATURES, name
-    assert lib.fvb_abi_version() == 1
+    assert lib.fvb_abi_version() == _native.ABI_VERSION == 2
 
 
 def _plan(width, height, layout, depth, quality, fps=(24, 1), tile=(256, 128)):
@@ -189,3 +189,39 @@ def test_batch_bucket_rounds_counts_up_by_at_most_a_quarter():
     b.passes = 0
     assert lib.fvb_bucket_encode_plan(ctypes.byref(b), ctypes.byref(ws)) == -1
     assert _native.last_error() == "invalid bucket"
+
+
+def test_bucket_folded_symbol_width():
+    """Folded symbols are held as u16 unless a frame is 16-bit lossless: the
+    bucket records it, the workspace shrinks by 2 bytes per sample, and a u32
+    capacity still takes a batch that would fit u16."""
+    from fastvid_b200._native import Bucket
+
+    lib = _native.load()
+
+    def bucket(specs):
+        frames = []
+        for w, h, layout, depth, q in specs:
+            rc, frame, _ = _plan(w, h, layout, depth, q)
+            assert rc == 0
+            frames.append(frame)
+        arr = (Frame * len(frames))(*frames)
+        b = Bucket()
+        assert lib.fvb_batch_bucket(arr, len(frames), ctypes.byref(b)) == 0
+        exact = ctypes.c_int64()
+        assert lib.fvb_batch_encode_plan(arr, len(frames), ctypes.byref(exact)) == 0
+        return b, exact.value, arr
+
+    b8, ws8, _ = bucket([(640, 360, 0, 8, 100), (320, 200, 2, 12, 100)])
+    assert b8.fold16 == 1
+    b16, _, _ = bucket([(640, 360, 0, 16, 99), (320, 200, 1, 16, 50)])
+    assert b16.fold16 == 1
+    bl, wsl, arr = bucket([(640, 360, 0, 8, 100), (320, 200, 2, 16, 100)])
+    assert bl.fold16 == 0
+    b8b, ws8b, _ = bucket([(640, 360, 0, 8, 100), (320, 200, 2, 16, 99)])
+    assert b8b.fold16 == 1 and wsl - ws8b >= 2 * (640 * 360 + 3 * 320 * 200)
+    # the u16 bucket refuses the lossless 16-bit batch; a u32 one takes a u16 batch
+    ws = ctypes.c_int64()
+    assert lib.fvb_bucket_encode_plan(ctypes.byref(b8b), ctypes.byref(ws)) == 0
+    b8b.fold16 = 0
+    assert lib.fvb_bucket_encode_plan(ctypes.byref(b8b), ctypes.byref(ws)) == 0

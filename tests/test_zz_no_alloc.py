@@ -57,7 +57,8 @@ def _encode(width, height, layout, depth, quality, tile, seed):
 
 def test_noalloc_decode_matches_workspace_decode_on_consecutive_calls(cuda):
     streams = [
-        _encode(1920, 1080, "rgb444", 8, 90, (64, 64), 101),   # 6.2 M samples, near the array's limit
+        _encode(1920, 1080, "rgb444", 8, 90, (64, 64), 101),   # 6.2 M samples
+        _encode(3840, 2160, "gray", 16, 87, (128, 128), 104),  # 8.3 M samples: fits with u16 folded symbols
         _encode(640, 360, "yuv422", 10, 80, (128, 128), 102),
         _encode(1280, 720, "gray", 16, 87, (128, 128), 103),
     ]
@@ -74,7 +75,12 @@ def test_noalloc_decode_matches_workspace_decode_on_consecutive_calls(cuda):
 def test_noalloc_decode_rejects_frames_beyond_its_scratch(cuda):
     lib = _native.load()
     assert lib.fvb_decode_noalloc_capacity() == 32 << 20
-    stream = _encode(3840, 2160, "gray", 16, 87, (128, 128), 104)  # 8.3 M samples
+    # 8.3 M samples of a lossless 16-bit frame: u32 folded symbols, beyond the array
+    stream = _encode(3840, 2160, "gray", 16, 100, (128, 128), 104)
+    rc, _ = _decode_noalloc(stream)
+    assert rc != 0
+    assert "allocation-free decode" in _native.last_error()
+    stream = _encode(3840, 2160, "rgb444", 8, 90, (128, 128), 106)  # 24.9 M samples
     rc, _ = _decode_noalloc(stream)
     assert rc != 0
     assert "allocation-free decode" in _native.last_error()
