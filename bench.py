@@ -695,8 +695,9 @@ def main():
                        "h2d_bytes_per_step": frame_bytes,
                        "d2h_bytes_per_step": stream_bytes + frame_bytes, "ms_per_step": e2e_ms,
                        "path": "BatchCodec.encode_decode_host: pinned frames in, pinned streams and decoded planes "
-                               "out; chunks of 8 frames, the upload of chunk i+3, the kernels of chunk i and the "
-                               "download of chunk i-1 overlapping",
+                               "out; chunks of at most 32 MB of samples, uploads running ahead into a ring of "
+                               "device buffers, encode on the calling stream and decode on a second host thread's "
+                               "stream, downloads overlapping the uploads",
                        "link": link, "copy_floor_frac": link["floor_ms"] / e2e_ms}
         roundtrip_ok = all(np.array_equal(o.numpy(), h) for op, hf, s in zip(out["planes"], host_frames, specs)
                            if s["quality"] == 100 for o, h in zip(op, hf))

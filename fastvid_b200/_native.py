@@ -70,6 +70,8 @@ SIGNATURES = {
     "fvb_get_decode_overlap": ([], c_i32),
     "fvb_set_rans_pipeline": ([c_i32], c_i32),
     "fvb_get_rans_pipeline": ([], c_i32),
+    "fvb_set_rans_pipeline_tail": ([c_i32], c_i32),
+    "fvb_get_rans_pipeline_tail": ([], c_i32),
     "fvb_profile_begin": ([], c_i32),
     "fvb_profile_end": ([c_p, c_p, c_i32], c_i32),
     "fvb_encode_plan": ([c_i64, c_i64, c_i32, c_i32, c_i32, c_i64, c_i64, c_i64, c_i64,

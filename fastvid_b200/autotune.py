@@ -138,14 +138,23 @@ def set_rans_pipeline(steps: int) -> None:
     _native.check(_native.load().fvb_set_rans_pipeline(int(steps)))
 
 
+def rans_pipeline_tail() -> int:
+    return int(_native.load().fvb_get_rans_pipeline_tail())
+
+
+def set_rans_pipeline_tail(steps: int) -> None:
+    _native.check(_native.load().fvb_set_rans_pipeline_tail(int(steps)))
+
+
 def apply(table: dict) -> None:
     """Set the table's launch geometry, wavefront block, warps per tile,
-    decode overlap and rANS encoder pipeline (process-wide)."""
+    decode overlap and rANS encoder pipelines (process-wide)."""
     set_launch(table.get("launch", {}))
     set_wavefront_block(table.get("wavefront_block", 0))
     set_tile_warps(table.get("tile_warps", 0))
     set_decode_overlap(table.get("decode_overlap", 1))
     set_rans_pipeline(table.get("rans_pipeline", 0))
+    set_rans_pipeline_tail(table.get("rans_pipeline_tail", 0))
 
 
 def tile_for(table: dict | None, layout: str, bit_depth: int, width: int, height: int, default=(256, 128)):
@@ -202,14 +211,16 @@ def tune_wavefront_block(codec, frames, params, candidates=WAVEFRONT_BLOCKS, rep
     return best, {str(k): round(v, 3) for k, v in seen.items()}
 
 
-def tune_rans_pipeline(codec, frames, params, reps: int = 3) -> tuple[int, dict]:
-    """The rANS encoder's fetch scheme (0, 8, 16) with the lowest batch time."""
+def tune_rans_pipeline(codec, frames, params, reps: int = 3, tail: bool = False) -> tuple[int, dict]:
+    """The rANS encoder's fetch scheme (0, 8, 16) with the lowest batch time,
+    for the first encoder pass or (tail) the later ones."""
+    setter = set_rans_pipeline_tail if tail else set_rans_pipeline
     seen = {}
     for steps in (0, 8, 16):
-        set_rans_pipeline(steps)
+        setter(steps)
         seen[steps] = _time_batch(codec, frames, params, reps)[0]
     best = min(seen, key=seen.get)
-    set_rans_pipeline(best)
+    setter(best)
     return best, {str(k): round(v, 3) for k, v in seen.items()}
 
 
@@ -285,6 +296,7 @@ def main(argv=None) -> int:
     block, block_ms = tune_wavefront_block(codec, frames, params, reps=args.reps)
     warps, warps_ms = tune_tile_warps(codec, frames, params, reps=args.reps)
     pipe, pipe_ms = tune_rans_pipeline(codec, frames, params, reps=args.reps)
+    pipe_tail, pipe_tail_ms = tune_rans_pipeline(codec, frames, params, reps=args.reps, tail=True)
     launch = tune_launch(codec, frames, params, reps=args.reps)
     overlap, overlap_ms = tune_decode_overlap(codec, frames, params, reps=args.reps)
     tuned_ms = _time_batch(codec, frames, params, args.reps)[0]
@@ -293,6 +305,7 @@ def main(argv=None) -> int:
              "wavefront_block": block, "wavefront_block_ms": block_ms,
              "tile_warps": warps, "tile_warps_ms": warps_ms,
              "rans_pipeline": pipe, "rans_pipeline_ms": pipe_ms,
+             "rans_pipeline_tail": pipe_tail, "rans_pipeline_tail_ms": pipe_tail_ms,
              "decode_overlap": overlap, "decode_overlap_ms": overlap_ms,
              "launch": launch, "launch_gain": {"default_ms": round(base_ms, 3), "tuned_ms": round(tuned_ms, 3)}}
     save(table, args.out)

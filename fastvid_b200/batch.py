@@ -80,6 +80,16 @@ class BatchCodec:
         self._pin_buf: torch.Tensor | None = None
         self.graph_kernels = 0  # kernels run by graph replays (launch_count() sees only direct launches)
 
+    def _pinned_heads(self, n: int) -> torch.Tensor:
+        """Pinned host buffer for n gathered 32-byte headers: the gather
+        kernel writes it directly, so the read does not queue behind
+        downloads in flight on other streams."""
+        buf = getattr(self, "_heads_pin", None)
+        if buf is None or buf.numel() < 32 * n:
+            buf = torch.empty(max(32 * n, 4096), dtype=torch.uint8).pin_memory()
+            self._heads_pin = buf
+        return buf[:32 * n]
+
     def workspace_bytes(self) -> int:
         """Device bytes of the resident workspace (0 when not resident)."""
         return self._ws_buf.numel() if self._ws_buf is not None else 0
@@ -295,10 +305,11 @@ class BatchCodec:
             if headers is not None and len(headers) == n and all(len(h) >= 32 for h in headers):
                 raw = b"".join(bytes(h[:32]) for h in headers)
             else:
-                heads = ctypes.create_string_buffer(32 * n)
+                heads = self._pinned_heads(n)
                 _native.check(self.lib.fvb_gather_headers(s_arr, l_arr, n, self._hdr_scratch.data_ptr(),
-                                                          self._hdr_scratch.numel(), heads, cur.cuda_stream))
-                raw = heads.raw
+                                                          self._hdr_scratch.numel(), heads.data_ptr(),
+                                                          cur.cuda_stream))
+                raw = heads.numpy().tobytes()
             plans, shapes, sizes = [], [], []
             for i, s in enumerate(dev_streams):
                 header = raw[32 * i:32 * i + 32]
@@ -494,7 +505,7 @@ class BatchCodec:
     def headers(self, streams) -> list[bytes]:
         """The 32-byte header of each stream (shorter streams: their bytes):
         CPU streams read in place, this device's streams with one gather
-        kernel and one copy for all of them."""
+        kernel for all of them, which writes pinned host memory directly."""
         out: list = [None] * len(streams)
         dev = []
         for i, s in enumerate(streams):
@@ -511,17 +522,20 @@ class BatchCodec:
                     self._hdr_scratch = torch.empty(max(need, 1 << 16), dtype=torch.uint8, device=self.device)
                 s_arr = (ctypes.c_void_p * n)(*[streams[i].contiguous().data_ptr() for i in dev])
                 l_arr = (ctypes.c_int64 * n)(*[streams[i].numel() for i in dev])
-                heads = ctypes.create_string_buffer(32 * n)
+                heads = self._pinned_heads(n)
                 _native.check(self.lib.fvb_gather_headers(s_arr, l_arr, n, self._hdr_scratch.data_ptr(),
-                                                          self._hdr_scratch.numel(), heads, cur.cuda_stream))
+                                                          self._hdr_scratch.numel(), heads.data_ptr(),
+                                                          cur.cuda_stream))
+                raw = heads.numpy().tobytes()
             for k, i in enumerate(dev):
-                out[i] = heads.raw[32 * k:32 * k + min(32, streams[i].numel())]
+                out[i] = raw[32 * k:32 * k + min(32, streams[i].numel())]
         return out
 
 
-    def encode_decode_host(self, frames, *, chunk: int = 32, chunk_bytes: int = 96 << 20, ahead: int = 3,
-                           predictor: str = "wavefront", out_streams: torch.Tensor | None = None,
-                           out_planes: torch.Tensor | None = None, **params):
+    def encode_decode_host(self, frames, *, chunk: int = 32, chunk_bytes: int = 32 << 20,
+                           ring_bytes: int = 8 << 30, predictor: str = "wavefront",
+                           out_streams: torch.Tensor | None = None, out_planes: torch.Tensor | None = None,
+                           **params):
         """Encode frames held in (preferably pinned) host memory and decode
         the streams again -- the round trip a codec evaluation makes -- with
         the streams and the decoded planes delivered in pinned host memory
@@ -529,19 +543,28 @@ class BatchCodec:
 
         The frames go through in chunks of consecutive frames, each closed
         once it holds `chunk` frames or its next frame would take it above
-        `chunk_bytes` of samples (a larger frame is a chunk of its own): the
-        upload of chunk i+ahead, the encode and decode of chunk i, and the
-        download of chunk i-1's streams and planes run at once, on two copy
-        streams beside the compute stream, so both directions of the host
-        link stay busy while the kernels run.  Chunks of similar byte size
-        keep the pipeline's fill and drain -- the first upload and the last
-        download, which nothing overlaps -- short whatever the frame mix.  Device buffers are resident: a ring of ahead+1
-        upload slots and of stream and plane arenas, kept by the codec and
-        reused chunk after chunk (events order each reuse after the work
-        that last read the slot), so the pipeline makes no allocation once
-        warm.  The streams stay on the device between the encode and the
+        `chunk_bytes` of samples (a larger frame is a chunk of its own).
+        Two host threads drive the GPU: this one uploads the chunks as far
+        ahead as the ring of device buffers allows and encodes chunk i on
+        the calling stream; a decode thread decodes the
+        encoded chunks on a stream of its own, through a second codec (its
+        own shape buckets and workspaces), and downloads each chunk's
+        streams and planes.  So the encoder's wait for its stream lengths
+        and the decoder's waits for headers and status words overlap
+        instead of adding up, and uploads, kernels and downloads of
+        different chunks run at once on the two copy streams and the two
+        compute streams.  Device buffers are resident: a ring of slots, each
+        an upload buffer, a stream arena and a plane arena for one chunk
+        (about 6 bytes per sample), as many as `ring_bytes` holds (at least
+        two, at most one per chunk), kept by the codec and reused chunk
+        after chunk (events order each reuse after the download of the
+        chunk that last used the slot), so the pipeline makes no allocation
+        once warm.  The streams stay on the device between the encode and the
         decode.  Streams equal encode()'s and planes decode()'s.  Returns
         (streams, planes), one entry per frame."""
+        import queue
+        import threading
+
         n = len(frames)
         if n == 0:
             return [], []
@@ -549,18 +572,25 @@ class BatchCodec:
         per = {k: _per_frame(v, n, k) for k, v in params.items()}
         bounds = _chunk_bounds([2 * sum(p.numel() for p in f) for f in frames], chunk, chunk_bytes)
         nchunks = len(bounds) - 1
-        slots = min(ahead + 1, nchunks)
         chunk_samples = [sum(p.numel() for f in frames[lo:hi] for p in f) for lo, hi in zip(bounds, bounds[1:])]
         max_samples = max(chunk_samples)
+        slots = max(2, min(nchunks, ring_bytes // (6 * max_samples + (64 << 10))))
+        ahead = slots - 1
+        decoder = self._decode_partner()
+        out_s: list = [None] * n
+        out_p: list = [None] * n
         with torch.cuda.device(self.device):
             comp = torch.cuda.current_stream(self.device)
             ring = self._ring(slots, max_samples)
-            h2d, d2h = ring["h2d"], ring["d2h"]
-            h2d.wait_stream(comp)
-            d2h.wait_stream(comp)
+            h2d, d2h, dstream = ring["h2d"], ring["d2h"], ring["dec"]
+            for st in (h2d, d2h, dstream):
+                st.wait_stream(comp)
             staged: dict = {}
             freed = [None] * slots        # event: the slot's upload buffer was last read (encode done)
-            drained = [None] * slots      # event: the slot's arenas were last read (download done)
+            drained = [None] * nchunks    # event: chunk i's arenas were last read (download done)
+            drained_ready = [threading.Event() for _ in range(nchunks)]
+            work: queue.Queue = queue.Queue()
+            failure: list = []
 
             def stage(i):
                 lo, hi = bounds[i], bounds[i + 1]
@@ -587,64 +617,109 @@ class BatchCodec:
                     return buf.narrow(0, cursor, count), cursor + count
                 return torch.empty(count, dtype=dtype, pin_memory=True), cursor
 
-            out_s, out_p = [], []
-            cur_s = cur_p = 0
-            for i in range(min(ahead, nchunks)):
-                stage(i)
-            for i in range(nchunks):
-                dev, ev = staged.pop(i)
-                k = i % slots
-                comp.wait_event(ev)
-                if drained[k] is not None:
-                    comp.wait_event(drained[k])
-                lo, hi = bounds[i], bounds[i + 1]
-                streams = self.encode(dev, arena=ring["streams"][k], **{kk: v[lo:hi] for kk, v in per.items()})
-                done_enc = torch.cuda.Event()
-                done_enc.record(comp)
-                freed[k] = done_enc
-                planes = self.decode(streams, predictor=predictor, arena=ring["planes"][k])
-                if i + ahead < nchunks:
-                    stage(i + ahead)
-                done = torch.cuda.Event()
-                done.record(comp)
-                s_total = sum(int(st.numel()) for st in streams)
-                p_total = sum(p.numel() for f in planes for p in f)
-                s_src = streams[0]._base if streams[0]._base is not None else streams[0]
-                p_src = planes[0][0]._base if planes[0][0]._base is not None else planes[0][0]
-                hs, cur_s = host_slice(out_streams, cur_s, s_total, torch.uint8)
-                hp, cur_p = host_slice(out_planes, cur_p, p_total, torch.uint16)
-                with torch.cuda.stream(d2h):
-                    d2h.wait_event(done)
-                    if s_src.data_ptr() != ring["streams"][k].data_ptr():
-                        s_src.record_stream(d2h)  # an arena of its own (the ring slot was too small)
-                    if p_src.data_ptr() != ring["planes"][k].data_ptr():
-                        p_src.record_stream(d2h)
-                    hs.copy_(s_src.reshape(-1).narrow(0, 0, s_total), non_blocking=True)
-                    hp.copy_(p_src.reshape(-1).narrow(0, 0, p_total), non_blocking=True)
-                    dr = torch.cuda.Event()
-                    dr.record(d2h)
-                drained[k] = dr
-                off = 0
-                for st in streams:
-                    out_s.append(hs.narrow(0, off, st.numel()))
-                    off += st.numel()
-                off = 0
-                for f in planes:
-                    views = []
-                    for p in f:
-                        views.append(hp.narrow(0, off, p.numel()).view(p.shape))
-                        off += p.numel()
-                    out_p.append(tuple(views))
+            def decode_side():
+                cur_s = cur_p = 0
+                try:
+                    with torch.cuda.device(self.device), torch.cuda.stream(dstream):
+                        while True:
+                            item = work.get()
+                            if item is None:
+                                return
+                            i, streams, enc_done = item
+                            k = i % slots
+                            lo = bounds[i]
+                            dstream.wait_event(enc_done)
+                            if i >= slots:  # the plane arena's last download
+                                dstream.wait_event(drained[i - slots])
+                            s_src = streams[0]._base if streams[0]._base is not None else streams[0]
+                            own_arena = s_src.data_ptr() != ring["streams"][k].data_ptr()
+                            if own_arena:  # the ring slot was too small: an arena of its own
+                                s_src.record_stream(dstream)
+                                s_src.record_stream(d2h)
+                            planes = decoder.decode(streams, predictor=predictor, arena=ring["planes"][k])
+                            done = torch.cuda.Event()
+                            done.record(dstream)
+                            s_total = sum(int(st.numel()) for st in streams)
+                            p_total = sum(p.numel() for f in planes for p in f)
+                            p_src = planes[0][0]._base if planes[0][0]._base is not None else planes[0][0]
+                            hs, cur_s = host_slice(out_streams, cur_s, s_total, torch.uint8)
+                            hp, cur_p = host_slice(out_planes, cur_p, p_total, torch.uint16)
+                            with torch.cuda.stream(d2h):
+                                d2h.wait_event(done)
+                                if p_src.data_ptr() != ring["planes"][k].data_ptr():
+                                    p_src.record_stream(d2h)
+                                hs.copy_(s_src.reshape(-1).narrow(0, 0, s_total), non_blocking=True)
+                                hp.copy_(p_src.reshape(-1).narrow(0, 0, p_total), non_blocking=True)
+                                dr = torch.cuda.Event()
+                                dr.record(d2h)
+                            drained[i] = dr
+                            drained_ready[i].set()
+                            off = 0
+                            for j, st in enumerate(streams):
+                                out_s[lo + j] = hs.narrow(0, off, st.numel())
+                                off += st.numel()
+                            off = 0
+                            for j, f in enumerate(planes):
+                                views = []
+                                for p in f:
+                                    views.append(hp.narrow(0, off, p.numel()).view(p.shape))
+                                    off += p.numel()
+                                out_p[lo + j] = tuple(views)
+                except BaseException as exc:  # reported by the calling thread
+                    failure.append(exc)
+                    for e in drained_ready:
+                        e.set()
+                    while work.get() is not None:
+                        pass
+
+            worker = threading.Thread(target=decode_side, name="fastvid-roundtrip-decode", daemon=True)
+            worker.start()
+            try:
+                for i in range(min(ahead, nchunks)):
+                    stage(i)
+                for i in range(nchunks):
+                    dev, ev = staged.pop(i)
+                    k = i % slots
+                    comp.wait_event(ev)
+                    if i >= slots:  # the stream arena: decoded and downloaded
+                        drained_ready[i - slots].wait()
+                        if failure:
+                            break
+                        comp.wait_event(drained[i - slots])
+                    lo, hi = bounds[i], bounds[i + 1]
+                    streams = self.encode(dev, arena=ring["streams"][k], **{kk: v[lo:hi] for kk, v in per.items()})
+                    enc_done = torch.cuda.Event()
+                    enc_done.record(comp)
+                    freed[k] = enc_done
+                    work.put((i, streams, enc_done))
+                    if i + ahead < nchunks:
+                        stage(i + ahead)
+            finally:
+                work.put(None)
+                worker.join()
+            if failure:
+                torch.cuda.synchronize(self.device)
+                raise failure[0]
             d2h.synchronize()
             comp.wait_stream(d2h)
+            comp.wait_stream(dstream)
         return out_s, out_p
+
+    def _decode_partner(self) -> "BatchCodec":
+        """A second codec on this device for the round trip's decode thread
+        (its own shape buckets, workspaces and header scratch)."""
+        p = getattr(self, "_partner", None)
+        if p is None:
+            p = BatchCodec(self.device, use_graphs=self.use_graphs, max_cached_shapes=self.max_cached)
+            self._partner = p
+        return p
 
     def _ring(self, slots: int, samples: int) -> dict:
         """Resident buffers of the host round trip: `slots` upload slots and
         plane arenas of `samples` uint16, stream arenas of 2 * `samples` +
         64 KiB bytes (a chunk whose streams are larger -- possible only for
         near-incompressible 16-bit content -- gets an arena of its own), and
-        the two copy streams."""
+        the two copy streams and the decode thread's compute stream."""
         r = getattr(self, "_ring_bufs", None)
         if r is None or r["slots"] < slots or r["samples"] < samples:
             r = {"slots": slots, "samples": samples,
@@ -652,7 +727,8 @@ class BatchCodec:
                  "streams": [torch.empty(2 * samples + (64 << 10), dtype=torch.uint8, device=self.device)
                              for _ in range(slots)],
                  "planes": [torch.empty(samples, dtype=torch.uint16, device=self.device) for _ in range(slots)],
-                 "h2d": torch.cuda.Stream(self.device), "d2h": torch.cuda.Stream(self.device)}
+                 "h2d": torch.cuda.Stream(self.device), "d2h": torch.cuda.Stream(self.device),
+                 "dec": torch.cuda.Stream(self.device)}
             self._ring_bufs = r
         return r
 

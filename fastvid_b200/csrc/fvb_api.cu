@@ -547,6 +547,24 @@ int device_of(const void* p) {
   return -1;
 }
 
+// The device's view of page-locked host memory (every cudaMallocHost /
+// cudaHostAlloc allocation is mapped under unified addressing), or nullptr
+// for pageable memory.  Small results (status words, stream lengths,
+// headers) are written there by a kernel instead of a device-to-host copy:
+// copies in that direction run in issue order on the copy engine, so a
+// small copy issued while a large download is in flight on another stream
+// would wait for all of it (measured on B200: a 64-byte copy waited for a
+// 512 MB one), whereas kernel stores to host memory do not queue there.
+void* host_mapped(void* p) {
+  if (!p) return nullptr;
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return attr.type == cudaMemoryTypeHost ? attr.devicePointer : nullptr;
+}
+
 int check_ws(void* ws, int64_t ws_bytes, size_t need) {
   if (!ws || ws_bytes < static_cast<int64_t>(need))
     return fail(FVB_ERR_WORKSPACE, "workspace is smaller than planned");
@@ -582,6 +600,7 @@ std::atomic<int> g_ctas[K_COUNT];
 std::atomic<int> g_wavefront_block{kDefaultWavefrontBlock};
 std::atomic<int> g_decode_overlap{1};
 std::atomic<int> g_rans_pipeline{0};
+std::atomic<int> g_rans_pipeline_tail{0};
 std::atomic<int> g_tile_warps{kDefaultTileWarps};
 
 int ctas(int kernel) {
@@ -670,6 +689,14 @@ int fvb_set_rans_pipeline(int steps) {
 }
 
 int fvb_get_rans_pipeline(void) { return g_rans_pipeline.load(std::memory_order_relaxed); }
+
+int fvb_set_rans_pipeline_tail(int steps) {
+  if (steps != 0 && steps != 8 && steps != 16) return fail(FVB_ERR_ARGUMENT, "rANS pipeline must be 0, 8 or 16");
+  g_rans_pipeline_tail.store(steps, std::memory_order_relaxed);
+  return FVB_OK;
+}
+
+int fvb_get_rans_pipeline_tail(void) { return g_rans_pipeline_tail.load(std::memory_order_relaxed); }
 
 int fvb_set_tile_warps(int warps) {
   if (warps == 0) warps = kDefaultTileWarps;
@@ -873,7 +900,7 @@ int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, 
     FVB_LAUNCHED("enc_analyze_kernel");
     {
       LaunchScope scope_(K_ENC_RANS, stream);
-      enc_rans_launch(g_rans_pipeline.load(std::memory_order_relaxed), f16,
+      enc_rans_launch((pass == 0 ? g_rans_pipeline : g_rans_pipeline_tail).load(std::memory_order_relaxed), f16,
                       static_cast<int>(ceil_div(nsh * 4 > 0 ? nsh * 4 : 1, 128)), stream, state, dims, pass, shards,
                       folded, rans);
     }
@@ -885,12 +912,14 @@ int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, 
     FVB_LAUNCHED("enc_scan_kernel");
   }
   int64_t* res_d = reinterpret_cast<int64_t*>(ws + L.results);
+  int64_t* direct = static_cast<int64_t*>(host_mapped(results));  // pinned: written by the kernel
   {
     LaunchScope scope_(K_RESULTS, stream);
-    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, dims, res_d, 0);
+    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, dims, direct ? direct : res_d, 0);
   }
   FVB_LAUNCHED("results_kernel");
-  if (results) FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
+  if (results && !direct)
+    FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
   return FVB_OK;
 }
 
@@ -1081,7 +1110,8 @@ int fvb_gather_headers(const uint8_t* const* streams, const int64_t* stream_lens
     table[n + i] = static_cast<uint64_t>(stream_lens[i]);
   }
   FVB_CUDA(cudaMemcpyAsync(ws, table.data(), 16 * static_cast<size_t>(n), cudaMemcpyHostToDevice, stream));
-  uint8_t* out_d = reinterpret_cast<uint8_t*>(ws + align_up(16 * static_cast<size_t>(n)));
+  uint8_t* direct = static_cast<uint8_t*>(host_mapped(headers));  // pinned: written by the kernel
+  uint8_t* out_d = direct ? direct : reinterpret_cast<uint8_t*>(ws + align_up(16 * static_cast<size_t>(n)));
   {
     LaunchScope scope_(K_RESULTS, stream);
     gather_headers_kernel<<<static_cast<int>(ceil_div(n * kHeaderBytes, 256)), 256, 0, stream>>>(
@@ -1089,7 +1119,8 @@ int fvb_gather_headers(const uint8_t* const* streams, const int64_t* stream_lens
         n, out_d);
   }
   FVB_LAUNCHED("gather_headers_kernel");
-  FVB_CUDA(cudaMemcpyAsync(headers, out_d, kHeaderBytes * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
+  if (!direct)
+    FVB_CUDA(cudaMemcpyAsync(headers, out_d, kHeaderBytes * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
   FVB_CUDA(cudaStreamSynchronize(stream));
   return FVB_OK;
 }
@@ -1254,12 +1285,14 @@ int decode_enqueue(const Totals& t, int wavefront, void* workspace, int64_t work
     FVB_LAUNCHED("dec_reconstruct_serial_kernel");
   }
   int64_t* res_d = reinterpret_cast<int64_t*>(ws + L.results);
+  int64_t* direct = static_cast<int64_t*>(host_mapped(results));  // pinned: written by the kernel
   {
     LaunchScope scope_(K_RESULTS, stream);
-    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, dims, res_d, 1);
+    results_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, dims, direct ? direct : res_d, 1);
   }
   FVB_LAUNCHED("results_kernel");
-  if (results) FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
+  if (results && !direct)
+    FVB_CUDA(cudaMemcpyAsync(results, res_d, 16 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream));
   return FVB_OK;
 }
 

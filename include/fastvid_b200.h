@@ -106,6 +106,12 @@ int fvb_get_decode_overlap(void);
  * each launch; no output depends on it (the autotuner's knob). */
 int fvb_set_rans_pipeline(int steps);
 int fvb_get_rans_pipeline(void);
+/* The same choice for the encoder passes after the first, which re-encode
+ * only the frames the frame policy retries (gray10 MED, gray16 step
+ * refinement): few shards, so the pass is one lane's chain of dependent
+ * steps long whatever the load, and fetching further ahead pays. */
+int fvb_set_rans_pipeline_tail(int steps);
+int fvb_get_rans_pipeline_tail(void);
 /* While profiling is on (per calling thread), every launch is bracketed by
  * CUDA events on its stream; fvb_profile_end waits for them and writes, per
  * kernel id, the summed milliseconds and the number of launches. */
@@ -170,8 +176,11 @@ int fvb_batch_encode_prepare(const fvb_frame* frames, int n, const uint16_t* con
                              void* cuda_stream);
 
 /* Enqueues every analysis pass; no host synchronisation, so it can be
- * captured into a CUDA graph.  Copies n result records (status, stream
- * length) into `results` (pinned host memory, 2 int64 per frame). */
+ * captured into a CUDA graph.  Writes n result records (status, stream
+ * length) into `results` (host memory, 2 int64 per frame).  Page-locked
+ * `results` (cudaMallocHost / cudaHostAlloc) is written by a kernel
+ * directly; other host memory gets a device-to-host copy, which queues
+ * behind any larger download in flight on another stream. */
 int fvb_batch_encode_enqueue(const fvb_frame* frames, int n, void* workspace, int64_t workspace_bytes,
                              int64_t* results, void* cuda_stream);
 
@@ -182,7 +191,8 @@ int fvb_batch_encode_emit(const fvb_frame* frames, int n, void* workspace, int64
                           uint8_t* const* outs, void* cuda_stream);
 
 /* Copies the 32-byte header of each device stream into host `headers`
- * (32 * n bytes) with one gather kernel and one copy, and waits for it.
+ * (32 * n bytes) with one gather kernel (which writes page-locked
+ * `headers` directly, other memory through one copy), and waits for it.
  * `scratch` is device memory of at least 16*n rounded up to 256, plus 32*n
  * bytes. */
 int fvb_gather_headers(const uint8_t* const* streams, const int64_t* stream_lens, int n, void* scratch,
@@ -197,7 +207,8 @@ int fvb_batch_decode_prepare(const fvb_frame* frames, int n, const uint8_t* cons
                              void* workspace, int64_t workspace_bytes, void* cuda_stream);
 
 /* Enqueues parse, entropy decode and reconstruction for every frame (graph
- * capturable) and copies one int64 status per frame into `results`. */
+ * capturable) and writes one record per frame (status, 0) into `results`,
+ * as fvb_batch_encode_enqueue does. */
 int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void* workspace,
                              int64_t workspace_bytes, int64_t* results, void* cuda_stream);
 

@@ -120,14 +120,20 @@ def test_decode_overlap_knob_round_trip_and_rejections():
 
 def test_rans_pipeline_knob_round_trip_and_rejections():
     lib = _native.load()
-    before = autotune.rans_pipeline()
+    before = autotune.rans_pipeline(), autotune.rans_pipeline_tail()
     try:
         for steps in (0, 8, 16):
             autotune.set_rans_pipeline(steps)
+            autotune.set_rans_pipeline_tail(16 - steps if steps else 8)
             assert autotune.rans_pipeline() == steps
+            assert autotune.rans_pipeline_tail() == (16 - steps if steps else 8)
         for bad in (4, 32, -1):
             assert lib.fvb_set_rans_pipeline(bad) == -1 and "rANS pipeline" in _native.last_error()
-        autotune.apply({"launch": {}, "rans_pipeline": 8})
-        assert autotune.rans_pipeline() == 8
+            assert lib.fvb_set_rans_pipeline_tail(bad) == -1 and "rANS pipeline" in _native.last_error()
+        autotune.apply({"launch": {}, "rans_pipeline": 8, "rans_pipeline_tail": 16})
+        assert autotune.rans_pipeline() == 8 and autotune.rans_pipeline_tail() == 16
+        autotune.apply({"launch": {}})
+        assert autotune.rans_pipeline() == 0 and autotune.rans_pipeline_tail() == 0
     finally:
-        autotune.set_rans_pipeline(before)
+        autotune.set_rans_pipeline(before[0])
+        autotune.set_rans_pipeline_tail(before[1])

@@ -213,16 +213,19 @@ def test_wavefront_knobs_keep_the_bytes(cuda, mixed, block):
         autotune.set_tile_warps(before[1])
 
 
-@pytest.mark.parametrize("pipe", [8, 16])
-def test_rans_pipeline_keeps_the_bytes(cuda, mixed, pipe):
-    """The pipelined rANS encoder fetch writes the oracle's streams."""
+@pytest.mark.parametrize("pipe,tail", [(8, 16), (16, 8), (0, 16)])
+def test_rans_pipeline_keeps_the_bytes(cuda, mixed, pipe, tail):
+    """The pipelined rANS encoder fetch, in the first pass and in the
+    later passes of the frame policy, writes the oracle's streams."""
     from fastvid_b200 import autotune
 
-    before = autotune.rans_pipeline()
+    before = autotune.rans_pipeline(), autotune.rans_pipeline_tail()
     try:
         autotune.set_rans_pipeline(pipe)
+        autotune.set_rans_pipeline_tail(tail)
         codec = BatchCodec(cuda, use_graphs=False)
         for f, st in zip(mixed, _encode(codec, mixed)):
-            assert bytes(st.cpu().numpy().tobytes()) == f["oracle"], pipe
+            assert bytes(st.cpu().numpy().tobytes()) == f["oracle"], (pipe, tail)
     finally:
-        autotune.set_rans_pipeline(before)
+        autotune.set_rans_pipeline(before[0])
+        autotune.set_rans_pipeline_tail(before[1])
