@@ -45,12 +45,14 @@ class Bucket(ctypes.Structure):
     _fields_ = [
         ("frames", c_i64), ("tiles", c_i64), ("shards", c_i64), ("samples", c_i64), ("prefix", c_i64),
         ("frames_p", c_i64 * 3), ("tiles_p", c_i64 * 3), ("shards_p", c_i64 * 3),
+        ("samples_p", c_i64 * 3), ("prefix_p", c_i64 * 3),
         ("passes", c_i32), ("wide", c_i32), ("fold16", c_i32), ("pad", c_i32),
     ]
 
     def key(self) -> tuple:
         return (self.frames, self.tiles, self.shards, self.samples, self.prefix, tuple(self.frames_p),
-                tuple(self.tiles_p), tuple(self.shards_p), self.passes, self.wide, self.fold16)
+                tuple(self.tiles_p), tuple(self.shards_p), tuple(self.samples_p), tuple(self.prefix_p), self.passes,
+                self.wide, self.fold16)
 
 
 # exported symbol -> (argtypes, restype)
@@ -97,6 +99,7 @@ SIGNATURES = {
                                   c_i32),
     "fvb_bucket_encode_enqueue": ([ctypes.POINTER(Bucket), c_p, c_i64, c_p, c_p], c_i32),
     "fvb_bucket_encode_emit": ([ctypes.POINTER(Bucket), ctypes.POINTER(Frame), c_i32, c_p, c_i64, c_p, c_p], c_i32),
+    "fvb_bucket_encode_headers": ([ctypes.POINTER(Bucket), c_p, c_i64, c_p, c_p], c_i32),
     "fvb_bucket_decode_prepare": ([ctypes.POINTER(Bucket), ctypes.POINTER(Frame), c_i32, c_p, c_p, c_p, c_p, c_p,
                                    c_i64, c_p], c_i32),
     "fvb_bucket_decode_enqueue": ([ctypes.POINTER(Bucket), c_i32, c_p, c_i64, c_p, c_p], c_i32),

@@ -43,6 +43,7 @@ class _Slot:
     workspace: torch.Tensor
     results: torch.Tensor            # pinned int64 [bucket.frames, 2]
     wavefront: bool = True
+    headers: torch.Tensor | None = None  # encode: pinned uint8 [bucket.frames * 32], written by a kernel
     graph: torch.cuda.CUDAGraph | None = None
     stream: torch.cuda.Stream | None = None
     kernels: int = 0                 # kernel launches captured in the graph
@@ -136,7 +137,8 @@ class BatchCodec:
         plan = self.lib.fvb_bucket_decode_plan if decode else self.lib.fvb_bucket_encode_plan
         _native.check(plan(ctypes.byref(bucket), ctypes.byref(ws)))
         workspace = self._workspace(ws.value)
-        slot = _Slot(bucket, ws.value, workspace, self._results(bucket.frames), wavefront)
+        slot = _Slot(bucket, ws.value, workspace, self._results(bucket.frames), wavefront,
+                     headers=None if decode else torch.empty(32 * bucket.frames, dtype=torch.uint8).pin_memory())
         if len(cache) >= self.max_cached:
             cache.pop(next(iter(cache)))
         cache[key] = slot
@@ -176,13 +178,15 @@ class BatchCodec:
         return (f.layout, f.bit_depth, f.quality, f.width, f.height, f.tile_w, f.tile_h, f.fps_num, f.fps_den)
 
     def encode(self, frames, *, layout=None, bit_depth=10, quality=90, frame_rate=(24, 1), tile_size=(256, 128),
-               arena: torch.Tensor | None = None):
+               arena: torch.Tensor | None = None, return_headers: bool = False):
         """Encode a list of frames (each a tuple of CUDA uint16 planes).
 
         Scalar arguments apply to every frame; lists give one value per frame.
         `arena`: a device uint8 buffer the streams are written into when it
         is large enough (the caller keeps it alive and unused meanwhile).
-        Returns a list of 1-D CUDA uint8 streams (views of one arena).
+        Returns a list of 1-D CUDA uint8 streams (views of one arena); with
+        `return_headers`, also the streams' 32-byte headers (bytes), which
+        decode(streams, headers=...) takes instead of reading them back.
         """
         frames = [tuple(f) if not isinstance(f, torch.Tensor) else (f,) for f in frames]
         n = len(frames)
@@ -232,8 +236,13 @@ class BatchCodec:
             q_arr = (ctypes.c_int64 * (3 * n))(*pitches)
             _native.check(self.lib.fvb_bucket_encode_prepare(bucket, arr, n, p_arr, q_arr, slot.workspace.data_ptr(),
                                                              slot.ws_bytes, cur.cuda_stream))
-            self._run_slot(slot, lambda h: _native.check(self.lib.fvb_bucket_encode_enqueue(
-                bucket, slot.workspace.data_ptr(), slot.ws_bytes, slot.results.data_ptr(), h)), cur)
+            def enqueue(h):
+                _native.check(self.lib.fvb_bucket_encode_enqueue(bucket, slot.workspace.data_ptr(), slot.ws_bytes,
+                                                                 slot.results.data_ptr(), h))
+                _native.check(self.lib.fvb_bucket_encode_headers(bucket, slot.workspace.data_ptr(), slot.ws_bytes,
+                                                                 slot.headers.data_ptr(), h))
+
+            self._run_slot(slot, enqueue, cur)
             cur.synchronize()
             res = slot.results[:n].tolist()
             for i, (status, _) in enumerate(res):
@@ -257,6 +266,9 @@ class BatchCodec:
             for length in lengths:
                 views.append(arena.narrow(0, off, length))
                 off += length
+            if return_headers:
+                raw = slot.headers[:32 * n].numpy().tobytes()
+                return views, [raw[32 * i:32 * i + 32] for i in range(n)]
         return views
 
     # ---- decode -----------------------------------------------------------
@@ -550,8 +562,8 @@ class BatchCodec:
         encoded chunks on a stream of its own, through a second codec (its
         own shape buckets and workspaces), and downloads each chunk's
         streams and planes.  So the encoder's wait for its stream lengths
-        and the decoder's waits for headers and status words overlap
-        instead of adding up, and uploads, kernels and downloads of
+        and the decoder's wait for its status words overlap instead of
+        adding up (the headers come with the encoder's results), and uploads, kernels and downloads of
         different chunks run at once on the two copy streams and the two
         compute streams.  Device buffers are resident: a ring of slots, each
         an upload buffer, a stream arena and a plane arena for one chunk
@@ -625,7 +637,7 @@ class BatchCodec:
                             item = work.get()
                             if item is None:
                                 return
-                            i, streams, enc_done = item
+                            i, streams, heads, enc_done = item
                             k = i % slots
                             lo = bounds[i]
                             dstream.wait_event(enc_done)
@@ -636,7 +648,8 @@ class BatchCodec:
                             if own_arena:  # the ring slot was too small: an arena of its own
                                 s_src.record_stream(dstream)
                                 s_src.record_stream(d2h)
-                            planes = decoder.decode(streams, predictor=predictor, arena=ring["planes"][k])
+                            planes = decoder.decode(streams, predictor=predictor, headers=heads,
+                                                    arena=ring["planes"][k])
                             done = torch.cuda.Event()
                             done.record(dstream)
                             s_total = sum(int(st.numel()) for st in streams)
@@ -687,11 +700,12 @@ class BatchCodec:
                             break
                         comp.wait_event(drained[i - slots])
                     lo, hi = bounds[i], bounds[i + 1]
-                    streams = self.encode(dev, arena=ring["streams"][k], **{kk: v[lo:hi] for kk, v in per.items()})
+                    streams, heads = self.encode(dev, arena=ring["streams"][k], return_headers=True,
+                                                 **{kk: v[lo:hi] for kk, v in per.items()})
                     enc_done = torch.cuda.Event()
                     enc_done.record(comp)
                     freed[k] = enc_done
-                    work.put((i, streams, enc_done))
+                    work.put((i, streams, heads, enc_done))
                     if i + ahead < nchunks:
                         stage(i + ahead)
             finally:

@@ -288,15 +288,18 @@ int ensure_smem_attrs() {
 // workspace layouts
 
 // Encoder passes a frame may need: gray10 frames with a step above 1 may
-// re-run with the MED predictor, gray16 frames with a step above 1 may refine
-// their step twice (encode.cu frame policy; the device decides whether a
-// later pass actually runs).
+// re-run with the MED predictor, gray16 frames with a step above 1 may try a
+// refined step (encode.cu frame policy, :812-847; the device decides whether
+// the second pass runs).  The reference re-encodes a gray16 frame a third
+// time, with the baseline step, when the refined step loses; here the second
+// pass writes its records to a region of its own, so the first pass's
+// records are still there and are emitted instead (identical bytes, one
+// pass fewer).
 int frame_passes(const fvb_frame& f) {
-  if (f.layout == 0 && f.bit_depth == 10 && f.step > 1) return 2;
-  if (f.layout == 0 && f.bit_depth == 16 && f.step > 1) return 3;
+  if (f.layout == 0 && (f.bit_depth == 10 || f.bit_depth == 16) && f.step > 1) return 2;
   return 1;
 }
-constexpr int kMaxPasses = 3;
+constexpr int kMaxPasses = 3;  // capacity of the per-pass arrays (two passes are used)
 
 // Work of a batch, or the capacity of a bucket of batches (layouts and
 // launch grids are sized by capacity; kernels read the actual counts from
@@ -311,6 +314,7 @@ struct Totals {
   // batch out with frames of more passes first, so these are prefixes
   int frames_p[kMaxPasses] = {0, 0, 0};
   int64_t tiles_p[kMaxPasses] = {0, 0, 0}, shards_p[kMaxPasses] = {0, 0, 0};
+  int64_t samples_p[kMaxPasses] = {0, 0, 0}, prefix_p[kMaxPasses] = {0, 0, 0};
 };
 
 Totals totals_of(const fvb_frame* frames, int n) {
@@ -331,6 +335,8 @@ Totals totals_of(const fvb_frame* frames, int n) {
       ++t.frames_p[p];
       t.tiles_p[p] += f.tiles;
       t.shards_p[p] += f.shards;
+      t.samples_p[p] += f.samples;
+      t.prefix_p[p] += f.prefix_bytes;
     }
   }
   return t;
@@ -370,7 +376,8 @@ bool fits(const Totals& a, const Totals& cap) {
       a.prefix > cap.prefix || a.passes != cap.passes || a.wide != cap.wide || (cap.fold16 && !a.fold16))
     return false;
   for (int p = 0; p < kMaxPasses; ++p)
-    if (a.frames_p[p] > cap.frames_p[p] || a.tiles_p[p] > cap.tiles_p[p] || a.shards_p[p] > cap.shards_p[p])
+    if (a.frames_p[p] > cap.frames_p[p] || a.tiles_p[p] > cap.tiles_p[p] || a.shards_p[p] > cap.shards_p[p] ||
+        a.samples_p[p] > cap.samples_p[p] || a.prefix_p[p] > cap.prefix_p[p])
       return false;
   return true;
 }
@@ -396,6 +403,8 @@ Totals bucket_of(const Totals& t) {
     b.frames_p[p] = t.frames_p[p] ? static_cast<int>(bucket_round(t.frames_p[p], 1)) : 0;
     b.tiles_p[p] = t.tiles_p[p] ? bucket_round(t.tiles_p[p], 16) : 0;
     b.shards_p[p] = t.shards_p[p] ? bucket_round(t.shards_p[p], 16) : 0;
+    b.samples_p[p] = t.samples_p[p] ? bucket_round(t.samples_p[p], 1 << 16) : 0;
+    b.prefix_p[p] = t.prefix_p[p] ? bucket_round(t.prefix_p[p], 1 << 12) : 0;
   }
   return b;
 }
@@ -411,6 +420,8 @@ void to_bucket(const Totals& t, fvb_bucket* b) {
     b->frames_p[p] = t.frames_p[p];
     b->tiles_p[p] = t.tiles_p[p];
     b->shards_p[p] = t.shards_p[p];
+    b->samples_p[p] = t.samples_p[p];
+    b->prefix_p[p] = t.prefix_p[p];
   }
   b->passes = t.passes;
   b->wide = t.wide ? 1 : 0;
@@ -428,11 +439,14 @@ int from_bucket(const fvb_bucket* b, Totals* t) {
   t->samples = b->samples;
   t->prefix = b->prefix;
   for (int p = 0; p < kMaxPasses; ++p) {
-    if (b->frames_p[p] < 0 || b->frames_p[p] > b->frames || b->tiles_p[p] < 0 || b->shards_p[p] < 0)
+    if (b->frames_p[p] < 0 || b->frames_p[p] > b->frames || b->tiles_p[p] < 0 || b->shards_p[p] < 0 ||
+        b->samples_p[p] < 0 || b->prefix_p[p] < 0)
       return fail(FVB_ERR_ARGUMENT, "invalid bucket");
     t->frames_p[p] = static_cast<int>(b->frames_p[p]);
     t->tiles_p[p] = b->tiles_p[p];
     t->shards_p[p] = b->shards_p[p];
+    t->samples_p[p] = b->samples_p[p];
+    t->prefix_p[p] = b->prefix_p[p];
   }
   t->passes = b->passes;
   t->wide = b->wide != 0;
@@ -440,8 +454,12 @@ int from_bucket(const fvb_bucket* b, Totals* t) {
   return FVB_OK;
 }
 
+// Records of encoder pass 0 and of the later passes (region "b", sized for
+// the frames that take part in pass 1: a prefix of the batch, so the same
+// global shard and sample indices address both regions).
 struct EncLayout {
-  size_t dims, frames, state, outs, queue, results, shards, folded, rans, prefix, recon, total;
+  size_t dims, frames, state, outs, queue, results, shards, folded, rans, prefix, recon;
+  size_t shards_b, folded_b, rans_b, prefix_b, total;
 };
 
 EncLayout enc_layout(const Totals& t) {
@@ -464,6 +482,11 @@ EncLayout enc_layout(const Totals& t) {
   w.rans = take(static_cast<size_t>(kRansScratchBytes) * t.shards);
   w.prefix = take(static_cast<size_t>(t.prefix));
   w.recon = take(t.wide ? 2 * static_cast<size_t>(t.samples) : 0);
+  const bool later = t.passes > 1;
+  w.shards_b = take(later ? sizeof(ShardInfo) * t.shards_p[1] : 0);
+  w.folded_b = take(later ? (t.fold16 ? 2 : 4) * static_cast<size_t>(t.samples_p[1]) : 0);
+  w.rans_b = take(later ? static_cast<size_t>(kRansScratchBytes) * t.shards_p[1] : 0);
+  w.prefix_b = take(later ? static_cast<size_t>(t.prefix_p[1]) : 0);
   w.total = o;
   return w;
 }
@@ -501,6 +524,19 @@ __global__ void gather_headers_kernel(const uint8_t* const* __restrict__ streams
   if (i >= n * kHeaderBytes) return;
   const int k = i / kHeaderBytes, b = i % kHeaderBytes;
   out[i] = b < lens[k] ? streams[k][b] : 0;
+}
+
+// The 32-byte header of every frame of an encoded batch, in the caller's
+// order, from the records region the frame emits (its final pass).
+__global__ void encode_headers_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
+                                      const BatchDims* __restrict__ dims, const uint8_t* __restrict__ prefix_a,
+                                      const uint8_t* __restrict__ prefix_b, uint8_t* __restrict__ out) {
+  const int n = dims->frames_p[0];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * kHeaderBytes) return;
+  const int k = i / kHeaderBytes, b = i % kHeaderBytes;
+  const FrameDesc& f = frames[k];
+  out[f.slot * kHeaderBytes + b] = (state[k].final_b ? prefix_b : prefix_a)[f.prefix_base + b];
 }
 
 __global__ void results_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
@@ -858,11 +894,7 @@ int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, 
   const FrameDesc* frames_d = reinterpret_cast<const FrameDesc*>(ws + L.frames);
   FrameState* state = reinterpret_cast<FrameState*>(ws + L.state);
   int* queue = reinterpret_cast<int*>(ws + L.queue);
-  ShardInfo* shards = reinterpret_cast<ShardInfo*>(ws + L.shards);
-  void* folded = ws + L.folded;  // u16 or u32 symbols (cap.fold16)
-  const bool f16 = cap.fold16;
-  uint8_t* rans = reinterpret_cast<uint8_t*>(ws + L.rans);
-  uint8_t* prefix = reinterpret_cast<uint8_t*>(ws + L.prefix);
+  const bool f16 = cap.fold16;  // u16 or u32 folded symbols
   uint16_t* recon = reinterpret_cast<uint16_t*>(ws + L.recon);
   const int n = cap.frames;
   {
@@ -870,10 +902,15 @@ int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, 
     enc_init_kernel<<<(n + 127) / 128, 128, 0, stream>>>(frames_d, state, dims);
   }
   FVB_LAUNCHED("enc_init_kernel");
-  // pass p covers the batch's first frames_p[p] frames (layout order)
+  // pass p covers the batch's first frames_p[p] frames (layout order); the
+  // later passes write region b
   for (int pass = 0; pass < cap.passes; ++pass) {
     const int nf = cap.frames_p[pass];
     const int64_t tiles = cap.tiles_p[pass], nsh = cap.shards_p[pass];
+    ShardInfo* shards = reinterpret_cast<ShardInfo*>(ws + (pass ? L.shards_b : L.shards));
+    void* folded = ws + (pass ? L.folded_b : L.folded);
+    uint8_t* rans = reinterpret_cast<uint8_t*>(ws + (pass ? L.rans_b : L.rans));
+    uint8_t* prefix = reinterpret_cast<uint8_t*>(ws + (pass ? L.prefix_b : L.prefix));
     FVB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), stream));
     {
       LaunchScope scope_(K_ENC_PREDICT, stream);
@@ -946,16 +983,21 @@ int encode_emit(const Totals& cap, const fvb_frame* frames, int n, void* workspa
   int64_t max_prefix = 0;
   for (int i = 0; i < n; ++i) max_prefix = frames[i].prefix_bytes > max_prefix ? frames[i].prefix_bytes : max_prefix;
   dim3 gp(static_cast<unsigned>(ceil_div(max_prefix, 256 * 4) > 64 ? 64 : ceil_div(max_prefix, 256 * 4)), n);
+  const FrameState* state = reinterpret_cast<const FrameState*>(ws + L.state);
   {
     LaunchScope scope_(K_ENC_PREFIX, stream);
-    enc_prefix_kernel<<<gp, 256, 0, stream>>>(frames_d, n, reinterpret_cast<const uint8_t*>(ws + L.prefix), outs_d);
+    enc_prefix_kernel<<<gp, 256, 0, stream>>>(frames_d, state, n, reinterpret_cast<const uint8_t*>(ws + L.prefix),
+                                              reinterpret_cast<const uint8_t*>(ws + L.prefix_b), outs_d);
   }
   FVB_LAUNCHED("enc_prefix_kernel");
   {
     LaunchScope scope_(K_ENC_EMIT, stream);
-    enc_emit_launch(cap.fold16, grid_for(t.shards, kWarpsPerCta, ctas(K_ENC_EMIT)), enc_emit_smem(), stream, frames_d,
-                    n, reinterpret_cast<const ShardInfo*>(ws + L.shards), t.shards, ws + L.folded,
-                    reinterpret_cast<const uint8_t*>(ws + L.rans), outs_d);
+    enc_emit_launch(cap.fold16, grid_for(t.shards, kWarpsPerCta, ctas(K_ENC_EMIT)), enc_emit_smem(), stream, state,
+                    EmitRegion{reinterpret_cast<const ShardInfo*>(ws + L.shards), ws + L.folded,
+                               reinterpret_cast<const uint8_t*>(ws + L.rans)},
+                    EmitRegion{reinterpret_cast<const ShardInfo*>(ws + L.shards_b), ws + L.folded_b,
+                               reinterpret_cast<const uint8_t*>(ws + L.rans_b)},
+                    t.shards, outs_d);
   }
   FVB_LAUNCHED("enc_emit_kernel");
   return FVB_OK;
@@ -1011,6 +1053,31 @@ int fvb_bucket_encode_emit(const fvb_bucket* bucket, const fvb_frame* frames, in
   const int rc = from_bucket(bucket, &cap);
   if (rc) return rc;
   return encode_emit(cap, frames, n, workspace, workspace_bytes, outs, cuda_stream);
+}
+
+int fvb_bucket_encode_headers(const fvb_bucket* bucket, void* workspace, int64_t workspace_bytes, uint8_t* headers,
+                              void* cuda_stream) {
+  DeviceGuard guard_;
+  Totals cap;
+  int rc = from_bucket(bucket, &cap);
+  if (rc) return rc;
+  if (!headers) return fail(FVB_ERR_ARGUMENT, "null argument");
+  const EncLayout L = enc_layout(cap);
+  rc = check_ws(workspace, workspace_bytes, L.total);
+  if (rc) return rc;
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  char* ws = static_cast<char*>(workspace);
+  uint8_t* direct = static_cast<uint8_t*>(host_mapped(headers));
+  if (!direct) return fail(FVB_ERR_ARGUMENT, "headers must be page-locked host memory");
+  {
+    LaunchScope scope_(K_RESULTS, stream);
+    encode_headers_kernel<<<static_cast<int>(ceil_div(cap.frames * kHeaderBytes, 256)), 256, 0, stream>>>(
+        reinterpret_cast<const FrameDesc*>(ws + L.frames), reinterpret_cast<const FrameState*>(ws + L.state),
+        reinterpret_cast<const BatchDims*>(ws + L.dims), reinterpret_cast<const uint8_t*>(ws + L.prefix),
+        reinterpret_cast<const uint8_t*>(ws + L.prefix_b), direct);
+  }
+  FVB_LAUNCHED("encode_headers_kernel");
+  return FVB_OK;
 }
 
 int fvb_encode_analyze(const fvb_frame* frame, const uint16_t* const* planes, const int64_t* pitches, void* workspace,

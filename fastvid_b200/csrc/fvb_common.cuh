@@ -107,7 +107,7 @@ struct FrameState {
   int32_t refined;     // header flag 0x80
   int32_t status;      // first error code
   int32_t pass;        // policy stage
-  int32_t pad;
+  int32_t final_b;     // the frame's records are those of the later pass (region b)
   int64_t payload;     // sum of record bytes of the last completed pass
   int64_t baseline_payload;
   int64_t stream_len;  // header + directory + records

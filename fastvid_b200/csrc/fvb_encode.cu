@@ -346,10 +346,12 @@ enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     const int fi = frame_of_tile(frames, nframes, t);
     const FrameDesc& f = frames[fi];
     FrameState& st = state[fi];
-    if (!st.active) continue;
     const TileGeo g = tile_geo(f, t - f.tile_base);
-    // shard records of this tile (encode.cu:753-759); with pairs the first
-    // warp writes them
+    // shard records of this tile (encode.cu:753-759), written for every
+    // frame of the pass, active or not: the later passes write a region of
+    // their own, and the analysis kernels read every record of the pass
+    // (frame index first) before they skip inactive frames; with pairs the
+    // first warp writes them
     if (!pairs || (warp & 1) == 0) {
       for (int j = lane; j < g.shard_count; j += 32) {
         ShardInfo& si = shards[f.shard_base + g.first_shard + j];
@@ -359,6 +361,7 @@ enc_predict_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
         si.frame = fi;
       }
     }
+    if (!st.active) continue;
     if (g.w > kFastMaxW) continue;  // wide tiles go through enc_predict_wide_kernel
     const int32_t step = st.step;
     const uint32_t magic = step > 1 ? static_cast<uint32_t>((0x100000000ull + step - 1) / step) : 0u;
@@ -1252,6 +1255,7 @@ enc_scan_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
     // frame policy
     const int64_t N = f.nsamples;
     int next = 0;  // 0 done, 1 run again
+    bool keep_a = false;  // the later pass lost: pass 0's records stand
     if (st.pass == 0) {
       st.baseline_payload = payload;
       if (f.layout == 0 && f.bit_depth == 10 && st.step > 1 && payload * 10 > N * 3) {
@@ -1270,19 +1274,23 @@ enc_scan_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
         }
       }
     } else if (st.pass == 1) {
+      // gray16 refined-step trial (its records are in region b)
       const int64_t b = st.baseline_payload;
       const bool direct = b < N / 10 || b > N / 2;
       if (direct || payload < N / 10) {
         st.refined = 1;
+        st.final_b = 1;
       } else {
+        // the reference re-encodes with the baseline step (encode.cu:840-845);
+        // pass 0's records in region a are exactly that encoding
         st.step = f.step0;
-        st.use_med = 0;
-        st.pass = 2;
-        next = 1;
+        keep_a = true;
       }
+    } else if (st.pass == 3) {
+      st.final_b = 1;  // gray10 MED re-run: always final
     }
-    st.payload = payload;
-    st.stream_len = f.prefix_bytes + payload;
+    st.payload = keep_a ? st.baseline_payload : payload;
+    st.stream_len = f.prefix_bytes + st.payload;
     // header (encode.cu:871-885) -- written every pass, the last one stands
     pre[0] = 'F';
     pre[1] = 'V';
@@ -1424,15 +1432,20 @@ __device__ __forceinline__ void put_words(uint32_t* buf, int pos, uint32_t v, in
 
 template <typename FoldT>
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
-enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardInfo* __restrict__ shards,
-                int64_t total_shards, const FoldT* __restrict__ folded,
-                const uint8_t* __restrict__ rans_scratch, uint8_t* const* __restrict__ outs) {
+enc_emit_kernel(const FrameState* __restrict__ state, EmitRegion ra, EmitRegion rb, int64_t total_shards,
+                uint8_t* const* __restrict__ outs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* buf = reinterpret_cast<EmitWarpSmem*>(smem_raw)[warp].buf;
   const int64_t warps_total = static_cast<int64_t>(gridDim.x) * kWarpsPerCta;
   for (int64_t s = static_cast<int64_t>(blockIdx.x) * kWarpsPerCta + warp; s < total_shards; s += warps_total) {
-    const ShardInfo& si = shards[s];
+    // the frame's records: pass 0's, or its later pass's (the shard record
+    // of pass 0 names the frame either way)
+    const bool from_b = state[ra.shards[s].frame].final_b != 0;
+    const EmitRegion& rg = from_b ? rb : ra;
+    const ShardInfo& si = rg.shards[s];
+    const FoldT* __restrict__ folded = static_cast<const FoldT*>(rg.folded);
+    const uint8_t* __restrict__ rans_scratch = rg.rans_scratch;
     const int mode = si.mode, k = si.param, body = si.body, n = si.count;
     const int rec_len = min(body + 3, kMaxRecordBytes);
     const int nwords = (rec_len + 3) >> 2;
@@ -1625,13 +1638,15 @@ enc_emit_kernel(const FrameDesc* __restrict__ frames, int nframes, const ShardIn
   }
 }
 
-// Header + directory bytes of every frame into its output buffer.
-__global__ void enc_prefix_kernel(const FrameDesc* __restrict__ frames, int nframes,
-                                  const uint8_t* __restrict__ prefix, uint8_t* const* __restrict__ outs) {
+// Header + directory bytes of every frame into its output buffer (from the
+// region whose records the frame emits).
+__global__ void enc_prefix_kernel(const FrameDesc* __restrict__ frames, const FrameState* __restrict__ state,
+                                  int nframes, const uint8_t* __restrict__ prefix, const uint8_t* __restrict__ prefix_b,
+                                  uint8_t* const* __restrict__ outs) {
   const int fi = blockIdx.y;
   if (fi >= nframes) return;
   const FrameDesc& f = frames[fi];
-  const uint8_t* src = prefix + f.prefix_base;
+  const uint8_t* src = (state[fi].final_b ? prefix_b : prefix) + f.prefix_base;
   uint8_t* dst = outs[fi];
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < f.prefix_bytes;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -1641,15 +1656,12 @@ __global__ void enc_prefix_kernel(const FrameDesc* __restrict__ frames, int nfra
 }  // namespace fvb
 
 namespace fvb {
-void enc_emit_launch(bool fold16, int grid, size_t smem, cudaStream_t stream, const FrameDesc* frames, int nframes,
-                     const ShardInfo* shards, int64_t total_shards, const void* folded, const uint8_t* rans_scratch,
-                     uint8_t* const* outs) {
+void enc_emit_launch(bool fold16, int grid, size_t smem, cudaStream_t stream, const FrameState* state,
+                     EmitRegion a, EmitRegion b, int64_t total_shards, uint8_t* const* outs) {
   if (fold16)
-    enc_emit_kernel<uint16_t><<<grid, kWarpsPerCta * 32, smem, stream>>>(
-        frames, nframes, shards, total_shards, static_cast<const uint16_t*>(folded), rans_scratch, outs);
+    enc_emit_kernel<uint16_t><<<grid, kWarpsPerCta * 32, smem, stream>>>(state, a, b, total_shards, outs);
   else
-    enc_emit_kernel<uint32_t><<<grid, kWarpsPerCta * 32, smem, stream>>>(
-        frames, nframes, shards, total_shards, static_cast<const uint32_t*>(folded), rans_scratch, outs);
+    enc_emit_kernel<uint32_t><<<grid, kWarpsPerCta * 32, smem, stream>>>(state, a, b, total_shards, outs);
 }
 
 cudaError_t enc_emit_set_smem(int bytes) {

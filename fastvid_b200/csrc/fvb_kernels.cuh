@@ -89,12 +89,18 @@ void enc_rans_launch(int pipe, bool fold16, int grid, cudaStream_t stream, const
                      const BatchDims* dims, int pass, ShardInfo* shards, const void* folded, uint8_t* rans_scratch);
 __global__ void enc_scan_kernel(const FrameDesc* frames, FrameState* state, const BatchDims* dims, int pass,
                                 ShardInfo* shards, uint8_t* prefix);
-void enc_emit_launch(bool fold16, int grid, size_t smem, cudaStream_t stream, const FrameDesc* frames, int nframes,
-                     const ShardInfo* shards, int64_t total_shards, const void* folded, const uint8_t* rans_scratch,
-                     uint8_t* const* outs);
+// Records of one encoder region: pass 0's, or the later pass's (region b,
+// indexed like pass 0's for the frames that took part in it).
+struct EmitRegion {
+  const ShardInfo* shards;
+  const void* folded;
+  const uint8_t* rans_scratch;
+};
+void enc_emit_launch(bool fold16, int grid, size_t smem, cudaStream_t stream, const FrameState* state,
+                     EmitRegion a, EmitRegion b, int64_t total_shards, uint8_t* const* outs);
 cudaError_t enc_emit_set_smem(int bytes);
-__global__ void enc_prefix_kernel(const FrameDesc* frames, int nframes, const uint8_t* prefix,
-                                  uint8_t* const* outs);
+__global__ void enc_prefix_kernel(const FrameDesc* frames, const FrameState* state, int nframes, const uint8_t* prefix,
+                                  const uint8_t* prefix_b, uint8_t* const* outs);
 
 // decoder: shards binned by mode (0 rANS, 1 Rice, 2 zero-run, 3 block pack);
 // counts from dims (entry 0)

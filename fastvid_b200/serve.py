@@ -222,14 +222,15 @@ class Server:
                  max_batch_frames: int = 64, max_batch_pixels: int = 200_000_000, backend=None,
                  warm_bytes: int | None = None):
         """warm_bytes: device memory each worker allocates and frees once at
-        start on its own stream (default: a quarter of the budget per
-        worker, at most 4 GiB), so outputs come from the allocator's cache.
+        start on its own stream (default: half the budget shared among the
+        workers, at most 8 GiB each), so outputs come from the allocator's
+        cache.
         Each worker also allocates its resident workspace for the largest
         batch it may run (max_batch_pixels) at start when all workers' fit
         in half the budget, so the workspace never grows mid-run."""
         self.backend = backend if backend is not None else CodecBackend(device if device is not None else "cuda")
         self.budget = int(memory_budget)
-        self.warm_bytes = (min(4 << 30, self.budget // (4 * workers)) if warm_bytes is None else int(warm_bytes))
+        self.warm_bytes = (min(8 << 30, self.budget // (2 * workers)) if warm_bytes is None else int(warm_bytes))
         self.presize_bytes = 0
         if hasattr(self.backend, "largest_workspace"):
             need = self.backend.largest_workspace(max_batch_pixels)
@@ -452,11 +453,16 @@ def report(records: list[Done], t0: float) -> dict:
 def run_open_loop(server: Server, items, rate: float | None, seed: int = 0, keep=()):
     """Submit `items` -- (kind, payload, params) -- at Poisson arrivals of
     `rate` per second (None: all at once).  Answers are dropped as they come
-    in, except those whose item index is in `keep`.  Returns (records of
-    these requests in item order, t0, {index: answer})."""
+    in, except those whose item index is in `keep`: a set of indices (the
+    answer is copied into new device memory) or a dict {index: destination}
+    of tensors (or tuples of tensors) of the answers' shapes, allocated
+    before the run, that the answer is copied into -- so keeping answers
+    allocates nothing while the server runs.  Returns (records of these
+    requests in item order, t0, {index: kept answer})."""
     import random
 
     rng = random.Random(seed)
+    into = dict(keep) if isinstance(keep, dict) else {}
     keep = set(keep)
     kept: dict = {}
     rids = []
@@ -470,19 +476,31 @@ def run_open_loop(server: Server, items, rate: float | None, seed: int = 0, keep
             if remaining[0] == 0:
                 all_done.set()
 
-    def copy(answer):
+    def copy(answer, dst=None):
         # an answer is a view of its batch's output arena; a copy lets the
-        # arena go back to the allocator
+        # arena go back to the allocator (the callback runs on the worker's
+        # thread, so the copy is ordered on the worker's stream before any
+        # reuse of the arena)
         if isinstance(answer, torch.Tensor):
-            return answer.clone()
+            if dst is None:
+                return answer.clone()
+            if dst.shape != answer.shape or dst.dtype != answer.dtype:
+                raise ValueError("kept answer does not match its destination")
+            return dst.copy_(answer)
         if isinstance(answer, tuple):
-            return tuple(copy(a) for a in answer)
+            return tuple(copy(a, None if dst is None else d) for a, d in zip(answer, dst or (None,) * len(answer)))
         return answer
+
+    devices = set()
 
     def keeper(i):
         def done(f):
             if f.exception() is None:
-                kept[i] = copy(f.result())
+                res = f.result()
+                kept[i] = copy(res, into.get(i))
+                for a in (res if isinstance(res, tuple) else (res,)):
+                    if isinstance(a, torch.Tensor) and a.is_cuda:
+                        devices.add(a.device)
         return done
 
     t0 = time.perf_counter()
@@ -500,6 +518,8 @@ def run_open_loop(server: Server, items, rate: float | None, seed: int = 0, keep
         fut.add_done_callback(answered)  # answers are released with their futures
     if items:
         all_done.wait()
+    for dev in devices:  # the kept copies are complete on return
+        torch.cuda.synchronize(dev)
     want = set(rids)
     with server._cv:
         got = {r.rid: r for r in server.completed if r.rid in want}

@@ -225,6 +225,7 @@ int fvb_batch_decode_enqueue(const fvb_frame* frames, int n, int wavefront, void
 typedef struct fvb_bucket {
   int64_t frames, tiles, shards, samples, prefix;
   int64_t frames_p[3], tiles_p[3], shards_p[3]; /* per encoder pass */
+  int64_t samples_p[3], prefix_p[3];            /* per encoder pass */
   int32_t passes, wide;
   int32_t fold16, pad; /* 1: folded symbols held as u16 (every frame below depth 16 or quality 100) */
 } fvb_bucket;
@@ -241,6 +242,13 @@ int fvb_bucket_encode_prepare(const fvb_bucket* bucket, const fvb_frame* frames,
                               const uint16_t* const* planes, const int64_t* pitches, void* workspace,
                               int64_t workspace_bytes, void* cuda_stream);
 int fvb_bucket_encode_enqueue(const fvb_bucket* bucket, void* workspace, int64_t workspace_bytes, int64_t* results,
+                              void* cuda_stream);
+/* After fvb_bucket_encode_enqueue, on the same stream: writes the 32-byte
+ * header of every frame (32 * n bytes, the caller's order) into page-locked
+ * host memory `headers` by a kernel, so a caller that decodes the streams
+ * next has them with the results -- no read of the streams' first bytes,
+ * no extra wait.  Graph capturable. */
+int fvb_bucket_encode_headers(const fvb_bucket* bucket, void* workspace, int64_t workspace_bytes, uint8_t* headers,
                               void* cuda_stream);
 int fvb_bucket_encode_emit(const fvb_bucket* bucket, const fvb_frame* frames, int n, void* workspace,
                            int64_t workspace_bytes, uint8_t* const* outs, void* cuda_stream);

@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 
 # (width, height, layout, depth, quality, tile, noise sd)
 SPECS = [
-    (320, 200, "gray", 16, 87, (64, 64), (40, 1)),     # three encoder passes
+    (320, 200, "gray", 16, 87, (64, 64), (40, 1)),     # a refined-step trial that loses
     (300, 170, "gray", 10, 85, (128, 64), (3, 1)),     # MED re-run candidate
     (263, 133, "rgb444", 10, 90, (256, 128), (3, 1)),
     (301, 203, "yuv422", 8, 80, (67, 35), (2, 1)),
@@ -229,3 +229,24 @@ def test_rans_pipeline_keeps_the_bytes(cuda, mixed, pipe, tail):
     finally:
         autotune.set_rans_pipeline(before[0])
         autotune.set_rans_pipeline_tail(before[1])
+
+
+def test_encoder_returns_the_stream_headers(cuda, mixed):
+    """encode(..., return_headers=True) hands back each stream's 32-byte
+    header (written by a kernel into pinned memory with the results), the
+    final pass's flags included; decoding with them equals decoding
+    without."""
+    for graphs in (False, True):
+        codec = BatchCodec(cuda, use_graphs=graphs)
+        frames = [tuple(torch.from_numpy(p).cuda() for p in f["planes"]) for f in mixed]
+        kw = dict(layout=[f["layout"] for f in mixed], bit_depth=[f["bit_depth"] for f in mixed],
+                  quality=[f["quality"] for f in mixed], tile_size=[f["tile"] for f in mixed])
+        for _ in range(2):  # eager, then (graphs) a replay
+            streams, heads = codec.encode(frames, return_headers=True, **kw)
+            assert len(heads) == len(streams)
+            for f, st, h in zip(mixed, streams, heads):
+                assert h == f["oracle"][:32] == bytes(st[:32].cpu().numpy().tobytes())
+            with_heads = codec.decode(streams, headers=heads)
+            without = codec.decode(streams)
+            for a, b in zip(with_heads, without):
+                assert all(torch.equal(x, y) for x, y in zip(a, b))
