@@ -264,9 +264,11 @@ int side_stream(SideStream** out) {
   return FVB_OK;
 }
 
-// batches of at least this many shards (about 4 million samples) decode
-// their non-rANS shards on the side stream
-constexpr int64_t kSideStreamShards = 1024;
+// batches of at least this many shards (about 256 thousand samples: a 720p
+// gray frame has 240) decode their non-rANS shards on the side stream, beside
+// the rANS shards; both kernels are latency-bound for a single frame, so
+// overlapping them shortens its decode
+constexpr int64_t kSideStreamShards = 64;
 
 int ensure_smem_attrs() {
   static bool done[64] = {false};

@@ -550,6 +550,82 @@ dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
   }
 }
 
+// A Rice lane's bits, first bit lowest, through a private ring of 16 words
+// in shared memory fed by cp.async (the LaneRing scheme): 12 words are copied
+// before the first code; take() moves the next word into the 64-bit buffer
+// whenever the buffer holds 32 bits or fewer -- branch-free, once per code --
+// and copies one more word for each word it takes, so the copies stay at
+// least 11 words ahead of the reads.  (Loading words straight into a queue of
+// registers made every refill wait for a load: moving a register whose load
+// is in flight waits for it, and the four lanes of a shard refill at
+// different codes, so a warp met a load latency at nearly every code.)  Words
+// past the lane's last byte are not copied; bits read there are garbage, and
+// every position is checked against the lane's bit count instead.
+struct RiceRing {
+  static constexpr int kWords = 16;
+  static constexpr int kFill = 12;
+  static constexpr int kInFlight = 10;  // a word is read at least 11 copy groups after its copy
+  uint32_t* ring;         // slot 0 of this lane (slots 32 words apart)
+  const uint32_t* words;  // aligned base of the lane's bytes
+  int last;               // last word holding a lane byte (-1: none)
+  int fetched;            // next word to copy
+  int next;               // next word to take into the buffer
+  uint64_t bits;          // buffered bits, next bit lowest (zeros above nbits)
+  int nbits;
+
+  __device__ void issue(int w) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(ring + (w & (kWords - 1)) * 32));
+    const int ok = w <= last;
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %2, 0;\n @p cp.async.ca.shared.global [%0], [%1], 4;\n}\n" ::"r"(sa),
+        "l"(words + w), "r"(ok)
+        : "memory");
+  }
+  __device__ void init(uint32_t* ring_smem, const uint8_t* p, int64_t len) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const int head = static_cast<int>(a & 3);
+    words = reinterpret_cast<const uint32_t*>(a - head);
+    ring = ring_smem;
+    last = len > 0 ? static_cast<int>((head + len - 1) >> 2) : -1;
+#pragma unroll
+    for (int i = 0; i < kFill; ++i) issue(i);
+    fetched = kFill;
+    cp_async_commit();
+    cp_async_wait<0>();
+    bits = ring[0] >> (8 * head);  // the first word's bytes before the lane are dropped
+    nbits = 32 - 8 * head;
+    next = 1;
+  }
+  // Takes the next word when 32 bits or fewer are buffered (afterwards at
+  // least 33 are, or the buffer was already fuller).
+  __device__ void take() {
+    const bool need = nbits <= 32;
+    cp_async_wait<kInFlight>();
+    const uint32_t w = ring[(next & (kWords - 1)) * 32];
+    bits |= need ? static_cast<uint64_t>(w) << nbits : 0ull;
+    nbits += need ? 32 : 0;
+    next += need;
+    if (need) issue(fetched);
+    fetched += need;
+    cp_async_commit();
+  }
+};
+
+// cnt zero symbols from p: element stores up to a 16-byte boundary, then
+// 16-byte stores, then the tail (a zero run of a shard is up to 4,096
+// symbols, written by one thread).
+template <typename FoldT>
+__device__ __forceinline__ void zero_fill(FoldT* p, int64_t cnt) {
+  constexpr int kPer = 16 / sizeof(FoldT);
+  int64_t i = 0;
+  const int head = static_cast<int>(((16 - (reinterpret_cast<uintptr_t>(p) & 15)) & 15) / sizeof(FoldT));
+  for (; i < head && i < cnt; ++i) p[i] = 0;
+  uint4* v = reinterpret_cast<uint4*>(p + i);
+  const int64_t nv = (cnt - i) / kPer;
+  for (int64_t j = 0; j < nv; ++j) v[j] = make_uint4(0, 0, 0, 0);
+  for (i += nv * kPer; i < cnt; ++i) p[i] = 0;
+}
+
 struct OtherGroupSm {
   int32_t boff[32], bwidth[32];
   int32_t valid;
@@ -563,6 +639,7 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
                  FoldT* __restrict__ folded) {
   const int64_t total_shards = dims->shards_p[0];
   __shared__ OtherGroupSm sm_all[4];
+  __shared__ uint32_t rice_rings[4][RiceRing::kWords * 32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   OtherGroupSm& sm = sm_all[warp];
   const int my_g = lane >> 2, my_l = lane & 3;
@@ -618,56 +695,48 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
           if (ok) {
             const int k = mode - 1;
             const uint32_t rmask = k ? (1u << k) - 1u : 0u;
-            ByteWindow win;
-            win.init(body + loff, llen);
+            const int64_t total = 8 * llen;  // bits of this lane
+            RiceRing rr;
+            rr.init(&rice_rings[warp][lane], body + loff, llen);
             int64_t pos = 0;
             for (int idx = my_l; idx < n && ok; idx += lc) {
+              // unary quotient: zeros up to the next one bit (decode.cu:63-125)
+              rr.take();
               uint32_t q = 0;
-              for (;;) {
-                if (win.nbits == 0) {
-                  win.refill();
-                  if (win.nbits == 0) {
-                    ok = false;
-                    break;
-                  }
+              while (rr.bits == 0) {  // every buffered bit is zero: a long quotient
+                q += rr.nbits;
+                pos += rr.nbits;
+                rr.nbits = 0;
+                if (pos >= total || q > maxf) {
+                  ok = false;
+                  break;
                 }
-                if (win.bits == 0) {
-                  q += win.nbits;
-                  pos += win.nbits;
-                  win.nbits = 0;
-                  if (q > maxf) {
-                    ok = false;
-                    break;
-                  }
-                  continue;
-                }
-                const int z = __ffsll(static_cast<long long>(win.bits)) - 1;
-                q += z;
-                const int used = z + 1;
-                win.bits = used == 64 ? 0 : win.bits >> used;
-                win.nbits -= used;
-                pos += used;
-                if (q > maxf) ok = false;
-                break;
+                rr.take();
               }
               if (!ok) break;
-              if (win.nbits < k) win.refill();
-              if (win.nbits < k) {
+              const int z = __ffsll(static_cast<long long>(rr.bits)) - 1;
+              q += z;
+              rr.bits = z == 63 ? 0ull : rr.bits >> (z + 1);
+              rr.nbits -= z + 1;
+              pos += z + 1;
+              if (pos > total || q > maxf) {  // the one bit lies past the lane, or the quotient is too large
                 ok = false;
                 break;
               }
-              const uint32_t r = static_cast<uint32_t>(win.bits) & rmask;
-              win.bits >>= k;
-              win.nbits -= k;
+              // k remainder bits
+              if (rr.nbits < k) rr.take();
+              const uint32_t r = static_cast<uint32_t>(rr.bits) & rmask;
+              rr.bits >>= k;
+              rr.nbits -= k;
               pos += k;
               const uint64_t v = (static_cast<uint64_t>(q) << k) + r;
-              if (v > maxf) {
+              if (pos > total || v > maxf) {
                 ok = false;
                 break;
               }
               out[idx] = fold_store<FoldT>(static_cast<uint32_t>(v));
-              if (win.nbits <= 32) win.refill();
             }
+            cp_async_wait<0>();  // no copy into the ring outlives the lane
             if (ok) {
               const int64_t used = (pos + 7) / 8;
               if (used != llen) ok = false;
@@ -714,7 +783,8 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
               err = true;
               break;
             }
-            for (int64_t i = 0; i < run; ++i) out[produced++] = 0;
+            zero_fill(out + produced, run);
+            produced += run;
           } else {
             const uint32_t value = (token + 1) / 2;
             if (value == 0 || value > maxf) {

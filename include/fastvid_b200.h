@@ -91,7 +91,7 @@ int fvb_get_wavefront_block(void);
  * Process-wide, read at each launch; no output depends on it. */
 int fvb_set_tile_warps(int warps);
 int fvb_get_tile_warps(void);
-/* Whether large decode batches (1024 shards or more) run dec_other (Rice,
+/* Whether decode batches of 64 shards or more run dec_other (Rice,
  * zero-run and block-pack shards) on a side stream beside dec_rans (1, the
  * default) or after it on the caller's stream (0).  No reference
  * counterpart; process-wide, read at each launch; no output depends on it
