@@ -284,8 +284,9 @@ struct LaneRing {
   }
   __device__ void ready() { cp_async_wait<0>(); }
   // The eight bytes at lane positions cur..cur+7, first byte in the top
-  // bits; cur advances by at most eight between calls.
-  __device__ uint64_t window(int cur) {
+  // bits of hi, the next four in lo; cur advances by at most eight between
+  // calls.
+  __device__ void window(int cur, uint32_t& hi_out, uint32_t& lo_out) {
     const int pos = head + cur;
     const int w = pos >> 2;
 #pragma unroll
@@ -298,9 +299,8 @@ struct LaneRing {
     const uint32_t a = ring[(w & (kWords - 1)) * 32], b = ring[((w + 1) & (kWords - 1)) * 32],
                    c = ring[((w + 2) & (kWords - 1)) * 32];
     const int sh = 8 * (pos & 3);
-    const uint32_t hi = __byte_perm(__funnelshift_r(a, b, sh), 0, 0x0123);
-    const uint32_t lo = __byte_perm(__funnelshift_r(b, c, sh), 0, 0x0123);
-    return (static_cast<uint64_t>(hi) << 32) | lo;
+    hi_out = __byte_perm(__funnelshift_r(a, b, sh), 0, 0x0123);
+    lo_out = __byte_perm(__funnelshift_r(b, c, sh), 0, 0x0123);
   }
 };
 
@@ -463,8 +463,10 @@ __device__ __forceinline__ void rans_decode_lane(const uint32_t* __restrict__ bc
   // renormalisation shifts in one byte when x < 2^23 and a second when
   // x < 2^15 (decode.cu:540-545), taken from the top of an eight-byte window
   // read ahead of the state chain; four steps use at most eight bytes.
-  // Reading past the lane is an error, found by the byte count.
-  auto step = [&](uint64_t& win, int idx) {
+  // Reading past the lane is an error, found by the byte count.  The window
+  // is two 32-bit words (whi, wlo), shifted by funnel shifts: a 64-bit
+  // variable shift costs several instructions on the state chain.
+  auto step = [&](uint32_t& whi, uint32_t& wlo, int idx) {
     const uint32_t slot = x & ((1u << kRansTableLog) - 1u);
     const uint32_t bw = bcol[(slot >> kBucketShift) * kColumns];
     // starts at offsets 1..r of the bucket survive the shift by 31 - r
@@ -473,21 +475,25 @@ __device__ __forceinline__ void rans_decode_lane(const uint32_t* __restrict__ bc
     out[idx] = static_cast<FoldT>(val_col[sym << LOG_S]);  // symbols below 511
     x = (fc >> 12) * (x >> kRansTableLog) + slot - (fc & ((1u << kRansTableLog) - 1u));
     const int nb = (x < kRansL) + (x < (kRansL >> 8));
-    x = __funnelshift_l(static_cast<uint32_t>(win >> 32), x, 8 * nb);
-    win <<= 8 * nb;
+    const uint32_t sh = 8u * static_cast<uint32_t>(nb);  // 0, 8 or 16
+    x = __funnelshift_l(whi, x, sh);
+    whi = __funnelshift_l(wlo, whi, sh);
+    wlo <<= sh;
     cur += nb;
   };
   int idx = my_l;
   for (; idx + 12 < n; idx += 16) {
-    uint64_t win = ring.window(cur);
-    step(win, idx);
-    step(win, idx + 4);
-    step(win, idx + 8);
-    step(win, idx + 12);
+    uint32_t whi, wlo;
+    ring.window(cur, whi, wlo);
+    step(whi, wlo, idx);
+    step(whi, wlo, idx + 4);
+    step(whi, wlo, idx + 8);
+    step(whi, wlo, idx + 12);
   }
   if (idx < n) {
-    uint64_t win = ring.window(cur);
-    for (; idx < n; idx += 4) step(win, idx);  // at most three steps
+    uint32_t whi, wlo;
+    ring.window(cur, whi, wlo);
+    for (; idx < n; idx += 4) step(whi, wlo, idx);  // at most three steps
   }
   cp_async_wait<0>();
 }
@@ -626,6 +632,103 @@ __device__ __forceinline__ void zero_fill(FoldT* p, int64_t cnt) {
   for (i += nv * kPer; i < cnt; ++i) p[i] = 0;
 }
 
+// A zero-run shard (decode.cu:237-295) decoded by the whole warp, 32 body
+// bytes per step, one per lane.  A byte without the 0x80 bit ends a token
+// (ballot); the lane holding a token's last byte gathers the token's bytes
+// from the lanes before it by shuffles, with the bytes of a token begun in an
+// earlier step carried over; the symbols of the step's tokens are placed by
+// a warp prefix sum.  Every check of the serial parser is made -- at most
+// five bytes, the fifth at most 0x0f, canonical length, a run no longer than
+// the symbols left, a value in 1..maxf, no token after the last symbol, no
+// partial token and no missing symbol at the end -- so a stream is accepted
+// exactly when the serial parser accepts it.  The shard's symbols are zeroed
+// first; value tokens then write theirs.  Warp-collective: every lane calls
+// it with the same arguments.  Returns whether the shard is valid.
+template <typename FoldT>
+__device__ bool zero_run_warp(const uint8_t* __restrict__ body, int64_t blen, int n, uint32_t maxf,
+                              FoldT* __restrict__ out, int lane) {
+  for (int i = lane; i < n; i += 32) out[i] = 0;
+  __syncwarp();
+  int produced = 0;        // symbols of the steps so far (warp-uniform)
+  uint32_t pend_val = 0;   // value bits of a token begun in an earlier step
+  int pend_used = 0;       // its bytes so far (capped at 6)
+  bool pend_bad = false;   // its fifth byte was above 0x0f, or it is too long
+  bool bad = false;
+  for (int64_t base = 0; base < blen && !bad; base += 32) {
+    const bool vld = base + lane < blen;
+    const uint32_t byte = vld ? body[base + lane] : 0u;
+    const uint32_t endm = __ballot_sync(kFull, vld && !(byte & 0x80u));
+    const int nvalid = static_cast<int>(min(static_cast<int64_t>(32), blen - base));
+    const bool is_end = (endm >> lane) & 1u;
+    const uint32_t below = endm & ((1u << lane) - 1u);
+    const int prev = below ? 31 - __clz(below) : -1;  // the previous token's end in this step
+    const bool carried = prev < 0;                    // the token began in an earlier step
+    const int here = lane - prev;                     // its bytes in this step
+    const int cu = carried ? pend_used : 0;
+    uint32_t tok = carried ? pend_val : 0u;
+    bool tb = carried && pend_bad;
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+      const uint32_t bt = __shfl_sync(kFull, byte, max(lane - t, 0));
+      const int p = cu + here - 1 - t;  // position of byte lane - t in the token
+      if (t < here && p < 5) {
+        tok |= (bt & 0x7fu) << (7 * p);
+        if (p == 4 && bt > 0x0fu) tb = true;
+      }
+    }
+    if (cu + here > 5) tb = true;
+    if (!tb && cu + here != varint_len(tok)) tb = true;
+    uint32_t cnt = 0;
+    if (is_end) {
+      if (tok & 1u) {
+        const uint32_t value = (tok + 1u) >> 1;  // u32 arithmetic as in the reference
+        if (value == 0u || value > maxf) tb = true;
+        cnt = 1;
+      } else {
+        cnt = min((tok >> 1) + 1u, static_cast<uint32_t>(n) + 1u);  // a run; longer than n fails below
+      }
+    }
+    uint32_t inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(kFull, inc, o);
+      if (lane >= o) inc += v;
+    }
+    const uint32_t start = static_cast<uint32_t>(produced) + inc - cnt;
+    if (is_end) {
+      if (start + cnt > static_cast<uint32_t>(n)) tb = true;  // a run past the end, or a token after it
+      if (!tb && (tok & 1u)) out[start] = fold_store<FoldT>((tok + 1u) >> 1);
+    }
+    bad = __any_sync(kFull, is_end && tb);
+    produced += static_cast<int>(__shfl_sync(kFull, inc, 31));
+    // bytes after the step's last token end begin (or continue) a token
+    const int last_end = endm ? 31 - __clz(endm) : -1;
+    const int tail = nvalid - 1 - last_end;
+    if (tail > 0) {
+      const int c0 = endm ? 0 : pend_used;
+      uint32_t v = endm ? 0u : pend_val;
+      bool pb = endm ? false : pend_bad;
+#pragma unroll
+      for (int t = 0; t < 5; ++t) {
+        const uint32_t bt = __shfl_sync(kFull, byte, min(last_end + 1 + t, 31));
+        const int p = c0 + t;
+        if (t < tail && p < 5) {
+          v |= (bt & 0x7fu) << (7 * p);
+          if (p == 4 && bt > 0x0fu) pb = true;
+        }
+      }
+      pend_val = v;
+      pend_used = min(c0 + tail, 6);
+      pend_bad = pb || c0 + tail > 5;
+    } else {
+      pend_val = 0;
+      pend_used = 0;
+      pend_bad = false;
+    }
+  }
+  return !bad && pend_used == 0 && produced == n;
+}
+
 struct OtherGroupSm {
   int32_t boff[32], bwidth[32];
   int32_t valid;
@@ -750,51 +853,20 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
         }
       }
     } else if (list == 2) {
-      // ---- zero-run -----------------------------------------------------------
-      if (my_l == 0 && s_mine >= 0 && live) {
-        int64_t cursor = 0, produced = 0;
-        bool err = false;
-        while (produced < n && !err) {
-          uint32_t token = 0;
-          int shift = 0, used = 0;
-          for (;;) {
-            if (cursor >= blen || used == 5) {
-              err = true;
-              break;
-            }
-            const uint8_t byte = body[cursor++];
-            if (used == 4 && byte > 0x0f) {
-              err = true;
-              break;
-            }
-            token |= static_cast<uint32_t>(byte & 0x7f) << shift;
-            ++used;
-            if ((byte & 0x80) == 0) break;
-            shift += 7;
-          }
-          if (err) break;
-          if (used != varint_len(token)) {
-            err = true;
-            break;
-          }
-          if ((token & 1) == 0) {
-            const int64_t run = static_cast<int64_t>(token / 2) + 1;
-            if (run > n - produced) {
-              err = true;
-              break;
-            }
-            zero_fill(out + produced, run);
-            produced += run;
-          } else {
-            const uint32_t value = (token + 1) / 2;
-            if (value == 0 || value > maxf) {
-              err = true;
-              break;
-            }
-            out[produced++] = fold_store<FoldT>(value);
-          }
-        }
-        if (err || cursor != blen) set_status(&state[fi].status, 1);
+      // ---- zero-run: the warp takes the shards one after another --------------
+      for (int k = 0; k < kGroup; ++k) {
+        const int64_t sk = __shfl_sync(kFull, s_mine, 4 * k);
+        if (sk < 0) continue;
+        const bool lk = __shfl_sync(kFull, live, 4 * k);
+        if (!lk) continue;
+        const int nk = __shfl_sync(kFull, n, 4 * k);
+        const int64_t bk = __shfl_sync(kFull, blen, 4 * k);
+        const int fk = __shfl_sync(kFull, fi, 4 * k);
+        const uint32_t mk = __shfl_sync(kFull, maxf, 4 * k);
+        const uint8_t* bodyk =
+            reinterpret_cast<const uint8_t*>(__shfl_sync(kFull, reinterpret_cast<uintptr_t>(body), 4 * k));
+        FoldT* outk = reinterpret_cast<FoldT*>(__shfl_sync(kFull, reinterpret_cast<uintptr_t>(out), 4 * k));
+        if (!zero_run_warp(bodyk, bk, nk, mk, outk, lane) && lane == 0) set_status(&state[fk].status, 1);
       }
     } else {
       // ---- block pack: the warp takes the shards one after another ------------

@@ -1034,7 +1034,10 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
   uint32_t* out_end = reinterpret_cast<uint32_t*>(base + kRansTableWords * 4 + kRansSerialBytes +
                                                   (lane + 1) * kRansLaneBytes);
   uint32_t x = kRansL;
-  uint64_t acc = 0;  // pending bytes, earliest emitted in the highest position
+  // pending bytes, earliest emitted in the highest position, as a 64-bit
+  // value in two words (ahi:alo) moved by funnel shifts: a 64-bit variable
+  // shift costs several instructions per step
+  uint32_t ahi = 0, alo = 0;
   int nacc = 0, nwords = 0;
   const int first = n - 1 - ((n - 1 - lane) & 3);
   const int steps = first >= 0 ? first / 4 + 1 : 0;  // symbols first, first-4, ..., >= 0
@@ -1046,13 +1049,15 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
     const uint32_t b1 = x >= thr, b2 = (x >> 8) >= thr;
     const int nb = static_cast<int>(b1 + b2);
     const uint32_t bytes = b2 ? __byte_perm(x, 0, 0x4401) : (x & 0xffu);  // first byte on top
-    acc = (acc << (8 * nb)) | (nb ? bytes : 0u);
+    const uint32_t sh = 8u * static_cast<uint32_t>(nb);  // 0, 8 or 16
+    ahi = __funnelshift_l(alo, ahi, sh);
+    alo = (alo << sh) | (nb ? bytes : 0u);
     nacc += nb;
     if (nacc >= 4) {
       nacc -= 4;
-      out_end[-(++nwords)] = static_cast<uint32_t>(acc >> (8 * nacc));
+      out_end[-(++nwords)] = __funnelshift_r(alo, ahi, 8 * nacc);  // (ahi:alo) >> 8 nacc, nacc 0 or 1
     }
-    x >>= 8 * nb;
+    x >>= sh;
     const uint32_t q = __umulhi(x, e.x) >> (e.y >> 25);
     x += (e.y & 0x1fffu) + q * cmpl;
   };
@@ -1112,7 +1117,7 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
     c = nblk * kB;
   }
   for (; c < steps; ++c) step(tab[ldf(f + first - 4 * c)]);
-  if (nacc) out_end[-(nwords + 1)] = static_cast<uint32_t>(acc << (8 * (4 - nacc)));  // low bytes unused
+  if (nacc) out_end[-(nwords + 1)] = alo << (8 * (4 - nacc));  // low bytes unused
   si.rans_lane[lane] = 4 * nwords + nacc;
   si.rans_state[lane] = x;
 }
