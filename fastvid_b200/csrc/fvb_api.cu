@@ -344,8 +344,9 @@ Totals totals_of(const fvb_frame* frames, int n) {
   return t;
 }
 
-// Encoder batch layout order: frames needing three passes, then two, then
-// one, each group in the caller's order.
+// Encoder batch layout order: frames that may need a second pass first, then
+// the rest, each group in the caller's order (the later passes run over a
+// prefix of the batch).
 std::vector<int> encode_order(const fvb_frame* frames, int n) {
   std::vector<int> order;
   order.reserve(n);

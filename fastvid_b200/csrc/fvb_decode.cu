@@ -803,37 +803,59 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
             rr.init(&rice_rings[warp][lane], body + loff, llen);
             int64_t pos = 0;
             for (int idx = my_l; idx < n && ok; idx += lc) {
-              // unary quotient: zeros up to the next one bit (decode.cu:63-125)
+              // unary quotient: zeros up to the next one bit, then k
+              // remainder bits (decode.cu:63-125)
               rr.take();
-              uint32_t q = 0;
-              while (rr.bits == 0) {  // every buffered bit is zero: a long quotient
-                q += rr.nbits;
-                pos += rr.nbits;
-                rr.nbits = 0;
-                if (pos >= total || q > maxf) {
+              const uint32_t lo = static_cast<uint32_t>(rr.bits);
+              const int z0 = __ffs(lo) - 1;  // -1: no one bit in the low word
+              uint64_t v;
+              if (z0 >= 0 && z0 + 1 + k <= rr.nbits) {
+                // the whole code is buffered and its quotient is below 32:
+                // one pass over it
+                const int tot = z0 + 1 + k;  // at most 48
+                const uint32_t r = __funnelshift_rc(lo, static_cast<uint32_t>(rr.bits >> 32), z0 + 1) & rmask;
+                rr.bits >>= tot;
+                rr.nbits -= tot;
+                pos += tot;
+                v = (static_cast<uint64_t>(z0) << k) + r;
+                if (pos > total || static_cast<uint32_t>(z0) > maxf) {  // the code runs past the lane
                   ok = false;
                   break;
                 }
-                rr.take();
+              } else {
+                uint32_t q = 0;
+                while (rr.bits == 0) {  // every buffered bit is zero: a long quotient
+                  q += rr.nbits;
+                  pos += rr.nbits;
+                  rr.nbits = 0;
+                  if (pos >= total || q > maxf) {
+                    ok = false;
+                    break;
+                  }
+                  rr.take();
+                }
+                if (!ok) break;
+                const int z = __ffsll(static_cast<long long>(rr.bits)) - 1;
+                q += z;
+                rr.bits = z == 63 ? 0ull : rr.bits >> (z + 1);
+                rr.nbits -= z + 1;
+                pos += z + 1;
+                if (pos > total || q > maxf) {  // the one bit lies past the lane, or the quotient is too large
+                  ok = false;
+                  break;
+                }
+                if (rr.nbits < k) rr.take();
+                const uint32_t r = static_cast<uint32_t>(rr.bits) & rmask;
+                rr.bits >>= k;
+                rr.nbits -= k;
+                pos += k;
+                v = (static_cast<uint64_t>(q) << k) + r;
+                if (pos > total) {
+                  ok = false;
+                  break;
+                }
               }
-              if (!ok) break;
-              const int z = __ffsll(static_cast<long long>(rr.bits)) - 1;
-              q += z;
-              rr.bits = z == 63 ? 0ull : rr.bits >> (z + 1);
-              rr.nbits -= z + 1;
-              pos += z + 1;
-              if (pos > total || q > maxf) {  // the one bit lies past the lane, or the quotient is too large
-                ok = false;
-                break;
-              }
-              // k remainder bits
-              if (rr.nbits < k) rr.take();
-              const uint32_t r = static_cast<uint32_t>(rr.bits) & rmask;
-              rr.bits >>= k;
-              rr.nbits -= k;
-              pos += k;
-              const uint64_t v = (static_cast<uint64_t>(q) << k) + r;
-              if (pos > total || v > maxf) {
+              if (v > maxf) {
                 ok = false;
                 break;
               }
