@@ -144,10 +144,11 @@ class BatchCodec:
         cache[key] = slot
         return slot
 
-    def _run_slot(self, slot: _Slot, enqueue, cur) -> None:
+    def _run_slot(self, slot: _Slot, enqueue, cur, graphs: bool = True) -> None:
         """Run `enqueue(stream_handle)` for this slot: captured as a graph on
-        the slot's first use (after one eager run), replayed afterwards."""
-        if not self.use_graphs:
+        the slot's first use (after one eager run), replayed afterwards;
+        launched directly when the codec or the call (`graphs`) says so."""
+        if not (self.use_graphs and graphs):
             enqueue(cur.cuda_stream)
             return
         if slot.graph is None:
@@ -178,7 +179,7 @@ class BatchCodec:
         return (f.layout, f.bit_depth, f.quality, f.width, f.height, f.tile_w, f.tile_h, f.fps_num, f.fps_den)
 
     def encode(self, frames, *, layout=None, bit_depth=10, quality=90, frame_rate=(24, 1), tile_size=(256, 128),
-               arena: torch.Tensor | None = None, return_headers: bool = False):
+               arena: torch.Tensor | None = None, return_headers: bool = False, graphs: bool = True):
         """Encode a list of frames (each a tuple of CUDA uint16 planes).
 
         Scalar arguments apply to every frame; lists give one value per frame.
@@ -187,6 +188,8 @@ class BatchCodec:
         Returns a list of 1-D CUDA uint8 streams (views of one arena); with
         `return_headers`, also the streams' 32-byte headers (bytes), which
         decode(streams, headers=...) takes instead of reading them back.
+        `graphs=False` launches directly even when the codec uses graphs (a
+        capture must not meet another thread's work on the device).
         """
         frames = [tuple(f) if not isinstance(f, torch.Tensor) else (f,) for f in frames]
         n = len(frames)
@@ -242,7 +245,7 @@ class BatchCodec:
                 _native.check(self.lib.fvb_bucket_encode_headers(bucket, slot.workspace.data_ptr(), slot.ws_bytes,
                                                                  slot.headers.data_ptr(), h))
 
-            self._run_slot(slot, enqueue, cur)
+            self._run_slot(slot, enqueue, cur, graphs)
             cur.synchronize()
             res = slot.results[:n].tolist()
             for i, (status, _) in enumerate(res):
@@ -276,11 +279,13 @@ class BatchCodec:
     def _dec_shape(f: Frame) -> tuple:
         return (f.layout, f.bit_depth, f.quality, f.flags, f.width, f.height, f.tile_w, f.tile_h)
 
-    def decode(self, streams, predictor="wavefront", headers=None, arena: torch.Tensor | None = None):
+    def decode(self, streams, predictor="wavefront", headers=None, arena: torch.Tensor | None = None,
+               graphs: bool = True):
         """Decode a list of 1-D uint8 streams; returns a list of plane tuples.
         `headers`: the streams' first 32 bytes when the caller has them
         (saves reading them back from the device).  `arena`: a device
-        uint16 buffer the planes are written into when it is large enough."""
+        uint16 buffer the planes are written into when it is large enough.
+        `graphs=False` launches directly even when the codec uses graphs."""
         if predictor not in ("wavefront", "serial"):
             raise ValueError("predictor must be 'wavefront' or 'serial'")
         n = len(streams)
@@ -366,7 +371,7 @@ class BatchCodec:
                                                              cur.cuda_stream))
             self._run_slot(slot, lambda h: _native.check(self.lib.fvb_bucket_decode_enqueue(
                 bucket, 1 if wavefront else 0, slot.workspace.data_ptr(), slot.ws_bytes, slot.results.data_ptr(),
-                h)), cur)
+                h)), cur, graphs)
             out_planes = []
             off = 0
             for f, _, samples, *_ in plans:
@@ -563,9 +568,11 @@ class BatchCodec:
         own shape buckets and workspaces), and downloads each chunk's
         streams and planes.  So the encoder's wait for its stream lengths
         and the decoder's wait for its status words overlap instead of
-        adding up (the headers come with the encoder's results), and uploads, kernels and downloads of
-        different chunks run at once on the two copy streams and the two
-        compute streams.  Device buffers are resident: a ring of slots, each
+        adding up (the headers come with the encoder's results).  Both
+        threads launch directly: a graph capture on one thread must not meet
+        the other thread's work on the device (a capture invalidated that
+        way was seen).  Uploads, kernels and downloads of different chunks
+        run at once on the two copy streams and the two compute streams.  Device buffers are resident: a ring of slots, each
         an upload buffer, a stream arena and a plane arena for one chunk
         (about 6 bytes per sample), as many as `ring_bytes` holds (at least
         two, at most one per chunk), kept by the codec and reused chunk
@@ -649,7 +656,7 @@ class BatchCodec:
                                 s_src.record_stream(dstream)
                                 s_src.record_stream(d2h)
                             planes = decoder.decode(streams, predictor=predictor, headers=heads,
-                                                    arena=ring["planes"][k])
+                                                    arena=ring["planes"][k], graphs=False)
                             done = torch.cuda.Event()
                             done.record(dstream)
                             s_total = sum(int(st.numel()) for st in streams)
@@ -700,7 +707,7 @@ class BatchCodec:
                             break
                         comp.wait_event(drained[i - slots])
                     lo, hi = bounds[i], bounds[i + 1]
-                    streams, heads = self.encode(dev, arena=ring["streams"][k], return_headers=True,
+                    streams, heads = self.encode(dev, arena=ring["streams"][k], return_headers=True, graphs=False,
                                                  **{kk: v[lo:hi] for kk, v in per.items()})
                     enc_done = torch.cuda.Event()
                     enc_done.record(comp)

@@ -250,3 +250,4 @@ def test_encoder_returns_the_stream_headers(cuda, mixed):
             without = codec.decode(streams)
             for a, b in zip(with_heads, without):
                 assert all(torch.equal(x, y) for x, y in zip(a, b))
+
