@@ -153,8 +153,8 @@ def apply(table: dict) -> None:
     set_wavefront_block(table.get("wavefront_block", 0))
     set_tile_warps(table.get("tile_warps", 0))
     set_decode_overlap(table.get("decode_overlap", 1))
-    set_rans_pipeline(table.get("rans_pipeline", 0))
-    set_rans_pipeline_tail(table.get("rans_pipeline_tail", 0))
+    set_rans_pipeline(table.get("rans_pipeline", -1))
+    set_rans_pipeline_tail(table.get("rans_pipeline_tail", -1))
 
 
 def tile_for(table: dict | None, layout: str, bit_depth: int, width: int, height: int, default=(256, 128)):
@@ -212,11 +212,12 @@ def tune_wavefront_block(codec, frames, params, candidates=WAVEFRONT_BLOCKS, rep
 
 
 def tune_rans_pipeline(codec, frames, params, reps: int = 3, tail: bool = False) -> tuple[int, dict]:
-    """The rANS encoder's fetch scheme (0, 8, 16) with the lowest batch time,
-    for the first encoder pass or (tail) the later ones."""
+    """The rANS encoder's fetch scheme (-1 automatic, 0, 8, 16) with the
+    lowest batch time, for the first encoder pass or (tail) the later ones;
+    the automatic choice wins ties."""
     setter = set_rans_pipeline_tail if tail else set_rans_pipeline
     seen = {}
-    for steps in (0, 8, 16):
+    for steps in (-1, 0, 8, 16):
         setter(steps)
         seen[steps] = _time_batch(codec, frames, params, reps)[0]
     best = min(seen, key=seen.get)

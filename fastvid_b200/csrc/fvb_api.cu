@@ -638,8 +638,19 @@ constexpr int kDefaultCtas[K_COUNT] = {
 std::atomic<int> g_ctas[K_COUNT];
 std::atomic<int> g_wavefront_block{kDefaultWavefrontBlock};
 std::atomic<int> g_decode_overlap{1};
-std::atomic<int> g_rans_pipeline{0};
-std::atomic<int> g_rans_pipeline_tail{0};
+// rANS encoder fetch scheme per pass: 0, 8, 16, or -1 (automatic: the
+// software pipeline over blocks of 8 steps when the launch leaves the SMs
+// short of warps -- a single frame, the frame policy's later passes -- where
+// the state chain would otherwise wait on its loads; the one-stage fetch,
+// which holds fewer registers, when the launch fills the GPU)
+std::atomic<int> g_rans_pipeline{-1};
+std::atomic<int> g_rans_pipeline_tail{-1};
+constexpr int kRansAutoCtasPerSm = 4;
+
+int rans_pipe_for(int knob, int grid) {
+  if (knob >= 0) return knob;
+  return grid <= device_sms() * kRansAutoCtasPerSm ? 8 : 0;
+}
 std::atomic<int> g_tile_warps{kDefaultTileWarps};
 
 int ctas(int kernel) {
@@ -722,7 +733,8 @@ int fvb_set_decode_overlap(int on) {
 int fvb_get_decode_overlap(void) { return g_decode_overlap.load(std::memory_order_relaxed); }
 
 int fvb_set_rans_pipeline(int steps) {
-  if (steps != 0 && steps != 8 && steps != 16) return fail(FVB_ERR_ARGUMENT, "rANS pipeline must be 0, 8 or 16");
+  if (steps != -1 && steps != 0 && steps != 8 && steps != 16)
+    return fail(FVB_ERR_ARGUMENT, "rANS pipeline must be -1, 0, 8 or 16");
   g_rans_pipeline.store(steps, std::memory_order_relaxed);
   return FVB_OK;
 }
@@ -730,7 +742,8 @@ int fvb_set_rans_pipeline(int steps) {
 int fvb_get_rans_pipeline(void) { return g_rans_pipeline.load(std::memory_order_relaxed); }
 
 int fvb_set_rans_pipeline_tail(int steps) {
-  if (steps != 0 && steps != 8 && steps != 16) return fail(FVB_ERR_ARGUMENT, "rANS pipeline must be 0, 8 or 16");
+  if (steps != -1 && steps != 0 && steps != 8 && steps != 16)
+    return fail(FVB_ERR_ARGUMENT, "rANS pipeline must be -1, 0, 8 or 16");
   g_rans_pipeline_tail.store(steps, std::memory_order_relaxed);
   return FVB_OK;
 }
@@ -940,9 +953,10 @@ int encode_enqueue(const Totals& cap, void* workspace, int64_t workspace_bytes, 
     FVB_LAUNCHED("enc_analyze_kernel");
     {
       LaunchScope scope_(K_ENC_RANS, stream);
-      enc_rans_launch((pass == 0 ? g_rans_pipeline : g_rans_pipeline_tail).load(std::memory_order_relaxed), f16,
-                      static_cast<int>(ceil_div(nsh * 4 > 0 ? nsh * 4 : 1, 128)), stream, state, dims, pass, shards,
-                      folded, rans);
+      const int grid = static_cast<int>(ceil_div(nsh * 4 > 0 ? nsh * 4 : 1, 128));
+      enc_rans_launch(rans_pipe_for((pass == 0 ? g_rans_pipeline : g_rans_pipeline_tail).load(std::memory_order_relaxed),
+                                    grid),
+                      f16, grid, stream, state, dims, pass, shards, folded, rans);
     }
     FVB_LAUNCHED("enc_rans_kernel");
     {

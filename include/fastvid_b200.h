@@ -102,8 +102,11 @@ int fvb_get_decode_overlap(void);
  * counterpart, whose lanes load as they go, cuda/csrc/encode.cu:398-418): 0
  * loads 16 symbols and then their table entries before each 16 steps; 8 or
  * 16 runs a software pipeline over blocks of that many steps, the symbols
- * two blocks and the table entries one block ahead.  Process-wide, read at
- * each launch; no output depends on it (the autotuner's knob). */
+ * two blocks and the table entries one block ahead; -1 (the default) picks
+ * per launch: the 8-step pipeline when the launch has at most 4 CTAs per SM
+ * (a single frame: its lanes' load latency is exposed), the one-stage fetch
+ * otherwise (it holds fewer registers).  Process-wide, read at each launch;
+ * no output depends on it (the autotuner's knob). */
 int fvb_set_rans_pipeline(int steps);
 int fvb_get_rans_pipeline(void);
 /* The same choice for the encoder passes after the first, which re-encode

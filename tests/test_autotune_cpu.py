@@ -127,13 +127,13 @@ def test_rans_pipeline_knob_round_trip_and_rejections():
             autotune.set_rans_pipeline_tail(16 - steps if steps else 8)
             assert autotune.rans_pipeline() == steps
             assert autotune.rans_pipeline_tail() == (16 - steps if steps else 8)
-        for bad in (4, 32, -1):
+        for bad in (4, 32, -2):
             assert lib.fvb_set_rans_pipeline(bad) == -1 and "rANS pipeline" in _native.last_error()
             assert lib.fvb_set_rans_pipeline_tail(bad) == -1 and "rANS pipeline" in _native.last_error()
         autotune.apply({"launch": {}, "rans_pipeline": 8, "rans_pipeline_tail": 16})
         assert autotune.rans_pipeline() == 8 and autotune.rans_pipeline_tail() == 16
-        autotune.apply({"launch": {}})
-        assert autotune.rans_pipeline() == 0 and autotune.rans_pipeline_tail() == 0
+        autotune.apply({"launch": {}})  # the automatic choice by default
+        assert autotune.rans_pipeline() == -1 and autotune.rans_pipeline_tail() == -1
     finally:
         autotune.set_rans_pipeline(before[0])
         autotune.set_rans_pipeline_tail(before[1])
