@@ -570,7 +570,7 @@ dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
 struct RiceRing {
   static constexpr int kWords = 16;
   static constexpr int kFill = 12;
-  static constexpr int kInFlight = 10;  // a word is read at least 11 copy groups after its copy
+  static constexpr int kInFlight = 10;  // a word is read at least 10 copy groups after its copy
   uint32_t* ring;         // slot 0 of this lane (slots 32 words apart)
   const uint32_t* words;  // aligned base of the lane's bytes
   int last;               // last word holding a lane byte (-1: none)
@@ -578,6 +578,7 @@ struct RiceRing {
   int next;               // next word to take into the buffer
   uint64_t bits;          // buffered bits, next bit lowest (zeros above nbits)
   int nbits;
+  uint32_t ahead;         // word `next`, read one take early so no code waits on the ring load
 
   __device__ void issue(int w) {
     const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(ring + (w & (kWords - 1)) * 32));
@@ -601,19 +602,26 @@ struct RiceRing {
     bits = ring[0] >> (8 * head);  // the first word's bytes before the lane are dropped
     nbits = 32 - 8 * head;
     next = 1;
+    ahead = ring[32];
   }
   // Takes the next word when 32 bits or fewer are buffered (afterwards at
   // least 33 are, or the buffer was already fuller).
+  // The word taken was read from the ring by the take before (or by init);
+  // the next one is read here, after the wait, for the take after: word w
+  // is copied by the take that takes word w - 11 and read by the one that
+  // takes word w - 1, ten copy groups later, so a wait leaving ten groups
+  // pending covers it.
   __device__ void take() {
     const bool need = nbits <= 32;
-    cp_async_wait<kInFlight>();
-    const uint32_t w = ring[(next & (kWords - 1)) * 32];
-    bits |= need ? static_cast<uint64_t>(w) << nbits : 0ull;
+    bits |= need ? static_cast<uint64_t>(ahead) << nbits : 0ull;
     nbits += need ? 32 : 0;
     next += need;
     if (need) issue(fetched);
     fetched += need;
     cp_async_commit();
+    cp_async_wait<kInFlight>();
+    const uint32_t w = ring[(next & (kWords - 1)) * 32];
+    ahead = need ? w : ahead;
   }
 };
 

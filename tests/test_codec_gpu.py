@@ -261,3 +261,51 @@ def test_mutated_streams_accepted_or_rejected_like_oracle(cuda, name):
             assert all(np.array_equal(g.cpu().numpy(), e) for g, e in zip(got, expected))
             accepted += 1
     assert rejected > 0
+
+
+def _sparse_gray8(width, height, seed):
+    rng = np.random.default_rng(seed)
+    plane = np.full((height, width), 128, dtype=np.uint16)
+    idx = rng.integers(0, width * height, size=width * height // 40)
+    plane.flat[idx] = rng.integers(0, 256, size=idx.size)
+    return (plane,)
+
+
+@pytest.mark.parametrize("kind", ["zero_run", "rice"])
+def test_mutated_zero_run_and_rice_payloads_like_oracle(cuda, kind):
+    """Mutations aimed at the payload of frames whose shards are zero-run
+    (sparse content) or Rice (noise): the warp-parallel zero-run parser and
+    the shared-memory Rice lanes accept or reject exactly as the serial
+    oracle does, and decode what they accept identically."""
+    if kind == "zero_run":
+        planes = _sparse_gray8(200, 96, 5)
+    else:
+        planes = synth.make_frame(200, 96, "gray", 8, 6, sigma=(3, 1))
+    tile = (64, 64)
+    folded, _, _ = oracle.predict(planes, layout="gray", bit_depth=8, tile_size=tile, step=1, use_med=0)
+    rows, _ = oracle.analyze(folded, width=200, height=96, layout="gray", tile_size=tile, force_order0=False)
+    modes = rows[:, 0]
+    assert ((modes == 0).sum() if kind == "zero_run" else ((modes >= 1) & (modes <= 17)).sum()) >= len(modes) // 2
+    stream = oracle.encode(planes, layout="gray", bit_depth=8, quality=100, tile_size=tile)
+    rng = np.random.default_rng(17 if kind == "zero_run" else 18)
+    payload0 = 32 + 32 * struct.unpack_from("<I", stream, 28)[0]
+    accepted = rejected = 0
+    for _ in range(160):
+        b = bytearray(stream)
+        for _ in range(int(rng.integers(1, 3))):
+            i = int(rng.integers(payload0, len(b)))
+            b[i] = int(rng.integers(0, 256)) if rng.random() < 0.5 else b[i] ^ (1 << int(rng.integers(0, 8)))
+        try:
+            expected = oracle.decode(bytes(b))
+        except oracle.OracleError:
+            expected = None
+        tensor = torch.frombuffer(bytearray(b), dtype=torch.uint8).cuda()
+        if expected is None:
+            with pytest.raises(RuntimeError):
+                fastvid_b200.decode(tensor)
+            rejected += 1
+        else:
+            got = fastvid_b200.decode(tensor)
+            assert all(np.array_equal(g.cpu().numpy(), e) for g, e in zip(got, expected))
+            accepted += 1
+    assert rejected > 0 and accepted > 0
