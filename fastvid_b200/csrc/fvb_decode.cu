@@ -810,27 +810,36 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
             RiceRing rr;
             rr.init(&rice_rings[warp][lane], body + loff, llen);
             int64_t pos = 0;
-            for (int idx = my_l; idx < n && ok; idx += lc) {
+            int idx = my_l;
+            while (idx < n && ok) {
               // unary quotient: zeros up to the next one bit, then k
               // remainder bits (decode.cu:63-125)
               rr.take();
-              const uint32_t lo = static_cast<uint32_t>(rr.bits);
-              const int z0 = __ffs(lo) - 1;  // -1: no one bit in the low word
-              uint64_t v;
+              uint32_t lo = static_cast<uint32_t>(rr.bits);
+              int z0 = __ffs(lo) - 1;  // -1: no one bit in the low word
               if (z0 >= 0 && z0 + 1 + k <= rr.nbits) {
-                // the whole code is buffered and its quotient is below 32:
-                // one pass over it
-                const int tot = z0 + 1 + k;  // at most 48
-                const uint32_t r = __funnelshift_rc(lo, static_cast<uint32_t>(rr.bits >> 32), z0 + 1) & rmask;
-                rr.bits >>= tot;
-                rr.nbits -= tot;
-                pos += tot;
-                v = (static_cast<uint64_t>(z0) << k) + r;
-                if (pos > total || static_cast<uint32_t>(z0) > maxf) {  // the code runs past the lane
-                  ok = false;
-                  break;
-                }
-              } else {
+                // codes wholly buffered, each with a quotient below 32: one
+                // pass over each, as many as the buffer holds
+                do {
+                  const int tot = z0 + 1 + k;  // at most 48
+                  const uint32_t r = __funnelshift_rc(lo, static_cast<uint32_t>(rr.bits >> 32), z0 + 1) & rmask;
+                  rr.bits >>= tot;
+                  rr.nbits -= tot;
+                  pos += tot;
+                  const uint64_t v = (static_cast<uint64_t>(z0) << k) + r;
+                  if (pos > total || v > maxf) {  // the code runs past the lane, or its value is too large
+                    ok = false;
+                    break;
+                  }
+                  out[idx] = fold_store<FoldT>(static_cast<uint32_t>(v));
+                  idx += lc;
+                  lo = static_cast<uint32_t>(rr.bits);
+                  z0 = __ffs(lo) - 1;
+                } while (idx < n && z0 >= 0 && z0 + 1 + k <= rr.nbits);
+                continue;
+              }
+              uint64_t v;
+              {
                 uint32_t q = 0;
                 while (rr.bits == 0) {  // every buffered bit is zero: a long quotient
                   q += rr.nbits;
@@ -868,6 +877,7 @@ dec_other_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ 
                 break;
               }
               out[idx] = fold_store<FoldT>(static_cast<uint32_t>(v));
+              idx += lc;
             }
             cp_async_wait<0>();  // no copy into the ring outlives the lane
             if (ok) {
