@@ -559,9 +559,10 @@ dec_rans_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict__ s
 // A Rice lane's bits, first bit lowest, through a private ring of 16 words
 // in shared memory fed by cp.async (the LaneRing scheme): 12 words are copied
 // before the first code; take() moves the next word into the 64-bit buffer
-// whenever the buffer holds 32 bits or fewer -- branch-free, once per code --
-// and copies one more word for each word it takes, so the copies stay at
-// least 11 words ahead of the reads.  (Loading words straight into a queue of
+// whenever the buffer holds 32 bits or fewer -- branch-free, once per refill
+// (the decoder then takes every code the buffer holds) -- and copies one more
+// word for each word it takes, so the copies stay at least 11 words ahead of
+// the word taken (10 ahead of the one read early).  (Loading words straight into a queue of
 // registers made every refill wait for a load: moving a register whose load
 // is in flight waits for it, and the four lanes of a shard refill at
 // different codes, so a warp met a load latency at nearly every code.)  Words
