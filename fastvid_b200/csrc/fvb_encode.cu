@@ -911,6 +911,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
     // order-0 rANS table (encode.cu:337-392), eligible when max < 511 and
     // at most 255 distinct symbols; one list entry per lane.
     const int rans_ok = shard_max < static_cast<uint32_t>(kRansAlphabet) && distinct <= 255;
+    bool rans_keep = false;
     if (rans_ok) {
       // Normalisation as a prefix maximum: for the i-th present symbol,
       // end_i = i + min(max(1, max_{j<=i}(f_j - j)), 4097 - D) with
@@ -930,6 +931,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
       const int head = 1 + varint_len(static_cast<uint32_t>(D));
       uint32_t c_count = 0, c_cursor = static_cast<uint32_t>(head);
       int32_t c_u = 1, c_end = 0, c_v = 0;
+      double info = 0.0;  // sum over the shard's symbols of log2(4096 / freq), this lane's entries
       for (int e0 = 0; e0 < D; e0 += 32) {
         const int e = e0 + lane;
         const bool ok = e < D;
@@ -965,6 +967,7 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
           if (lane >= o) binc += t;
         }
         if (ok) {
+          info += static_cast<double>(ent >> 16) * (static_cast<double>(kRansTableLog) - log2(static_cast<double>(fr)));
           tab[2 * v] = rans_multiplier(fr);
           tab[2 * v + 1] = rans_packed(fr, static_cast<uint32_t>(pe));
           uint32_t cursor = c_cursor + binc - bytes;
@@ -1003,8 +1006,22 @@ enc_analyze_kernel(const FrameDesc* __restrict__ frames, FrameState* __restrict_
         } while (d);
         si.rans_table = static_cast<int32_t>(c_cursor);
       }
+      // Skip the trial encoding when it cannot win.  Each rANS step takes a
+      // state x in [f 2^11, f 2^19) after renormalisation to one at least
+      // (x 4096 / f)(1 - 2^-11), and renormalising by b bytes keeps at least
+      // (x / 2^8b)(1 - 2^-11) of it; a lane starts at 2^23 and ends below
+      // 2^31.  So the bytes of the four lanes are at least
+      // (I - 4 * 8 - 2 n log2(1/(1 - 2^-11))) / 8 >= (I - 38) / 8 for
+      // I = sum log2(4096 / f) over the shard's n <= 4096 symbols, and with
+      // a 64-bit margin for rounding, table + 28 + floor((I - 64) / 8) is a
+      // lower bound of the rANS body.  When it reaches the best other body,
+      // rANS cannot be chosen (encode.cu:420-430 takes it only when smaller,
+      // or when the frame forces it) -- the bytes are the same without it.
+      for (int o = 16; o > 0; o >>= 1) info += __shfl_xor_sync(kFull, info, o);
+      const double bound = static_cast<double>(c_cursor) + 28.0 + floor((info - 64.0) / 8.0);
+      rans_keep = frames[frame].force_order0 || bound < static_cast<double>(body);
     }
-    if (lane == 0) si.rans_ok = rans_ok;
+    if (lane == 0) si.rans_ok = rans_ok && rans_keep;
     clear_bins();
   }
   cp_async_wait<0>();
