@@ -1011,9 +1011,9 @@ int encode_emit(const Totals& cap, const fvb_frame* frames, int n, void* workspa
     LaunchScope scope_(K_ENC_EMIT, stream);
     enc_emit_launch(cap.fold16, grid_for(t.shards, kWarpsPerCta, ctas(K_ENC_EMIT)), enc_emit_smem(), stream, state,
                     EmitRegion{reinterpret_cast<const ShardInfo*>(ws + L.shards), ws + L.folded,
-                               reinterpret_cast<const uint8_t*>(ws + L.rans)},
+                               reinterpret_cast<const uint8_t*>(ws + L.rans), t.shards},
                     EmitRegion{reinterpret_cast<const ShardInfo*>(ws + L.shards_b), ws + L.folded_b,
-                               reinterpret_cast<const uint8_t*>(ws + L.rans_b)},
+                               reinterpret_cast<const uint8_t*>(ws + L.rans_b), t.passes > 1 ? t.shards_p[1] : 0},
                     t.shards, outs_d);
   }
   FVB_LAUNCHED("enc_emit_kernel");

@@ -143,13 +143,17 @@ struct EncBand {
 #pragma unroll
       for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && col < W) ? __ldg(p + static_cast<int64_t>(r) * pitch) : 0u;
     }
-#pragma unroll
-    for (int r = 0; r < 32; ++r) vmax = max(vmax, pf[r]);
   }
+  // Every loaded chunk is stored once, a wavefront block after its load was
+  // issued; the depth check's maximum is taken here, where the loads have
+  // landed, not right after they are issued.
   __device__ void store_chunk(int k) {
     const int pj = k * 32 + lane;
 #pragma unroll
-    for (int r = 0; r < 32; ++r) sm.src[r * kSrcStride + ((pj + r) & 63)] = static_cast<uint16_t>(pf[r]);
+    for (int r = 0; r < 32; ++r) {
+      vmax = max(vmax, pf[r]);
+      sm.src[r * kSrcStride + ((pj + r) & 63)] = static_cast<uint16_t>(pf[r]);
+    }
   }
   __device__ void flush_chunk(int k) {
     const int col = k * 32 + lane;
@@ -229,13 +233,16 @@ __device__ void enc_tile_fast(const FrameDesc& f, const TileGeo& g, int32_t step
 #pragma unroll
         for (int r = 0; r < 32; ++r) pf[r] = (r < band_rows && col < W) ? __ldg(p + static_cast<int64_t>(r) * pitch) : 0u;
       }
-#pragma unroll
-      for (int r = 0; r < 32; ++r) vmax = max(vmax, pf[r]);
     };
+    // the depth check's maximum where the loads have landed (each loaded
+    // chunk is stored once, a wavefront block after its loads were issued)
     auto store_chunk = [&](int k) {
       const int pj = k * 32 + lane;
 #pragma unroll
-      for (int r = 0; r < 32; ++r) sm.src[r * kSrcStride + ((pj + r) & 63)] = static_cast<uint16_t>(pf[r]);
+      for (int r = 0; r < 32; ++r) {
+        vmax = max(vmax, pf[r]);
+        sm.src[r * kSrcStride + ((pj + r) & 63)] = static_cast<uint16_t>(pf[r]);
+      }
     };
     auto flush_chunk = [&](int k) {
       const int col = k * 32 + lane;
@@ -1462,13 +1469,19 @@ enc_emit_kernel(const FrameState* __restrict__ state, EmitRegion ra, EmitRegion 
   const int64_t warps_total = static_cast<int64_t>(gridDim.x) * kWarpsPerCta;
   for (int64_t s = static_cast<int64_t>(blockIdx.x) * kWarpsPerCta + warp; s < total_shards; s += warps_total) {
     // the frame's records: pass 0's, or its later pass's (the shard record
-    // of pass 0 names the frame either way)
-    const bool from_b = state[ra.shards[s].frame].final_b != 0;
-    const EmitRegion& rg = from_b ? rb : ra;
-    const ShardInfo& si = rg.shards[s];
-    const FoldT* __restrict__ folded = static_cast<const FoldT*>(rg.folded);
-    const uint8_t* __restrict__ rans_scratch = rg.rans_scratch;
+    // of pass 0 names the frame either way).  Frames with a later pass come
+    // first, so shards past region b's count skip the frame lookup.
+    const bool from_b = s < rb.count && state[ra.shards[s].frame].final_b != 0;
+    const ShardInfo& si = (from_b ? rb.shards : ra.shards)[s];
+    {  // the next shard's record into L1 while this one is assembled
+      const int64_t sn = s + warps_total;
+      if (lane < 2 && sn < total_shards)
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(reinterpret_cast<const char*>(ra.shards + sn) + 64 * lane));
+    }
+    const FoldT* __restrict__ folded = static_cast<const FoldT*>(from_b ? rb.folded : ra.folded);
+    const uint8_t* __restrict__ rans_scratch = from_b ? rb.rans_scratch : ra.rans_scratch;
     const int mode = si.mode, k = si.param, body = si.body, n = si.count;
+    uint8_t* const dst_base = outs[si.frame];  // loaded now, used at the copy-out
     const int rec_len = min(body + 3, kMaxRecordBytes);
     const int nwords = (rec_len + 3) >> 2;
     // clear words 0 .. nwords (one past the record: the copy-out reads it)
@@ -1479,33 +1492,55 @@ enc_emit_kernel(const FrameState* __restrict__ state, EmitRegion ra, EmitRegion 
     if (mode == kModeZeroRun) {
       // Tokens in symbol order (encode.cu:514-536): a zero run of length L is
       // varint(2(L-1)), a value v is varint(2v-1).  A run's token is written
-      // just before the value that ends it, or at the last symbol.
+      // just before the value that ends it, or at the last symbol.  The warp
+      // takes 128 symbols at a time, lane j holding symbols 4j..4j+3: the
+      // zero run reaching a lane starts after the last nonzero symbol of the
+      // lanes below (a ballot and one shuffle), the lane walks its four
+      // symbols twice (token lengths, then bytes), and one warp scan of the
+      // lengths places every lane's tokens.  The next 128 symbols are loaded
+      // while these are placed.
       int cursor = 3;
       int run_start = 0;  // first index of the zero run reaching the chunk start
-      const int nchunk = (n + 31) >> 5;
-      uint32_t v_next = lane < n ? ldf(f + lane) : 1u;  // loaded one chunk ahead
-      for (int m = 0; m < nchunk; ++m) {
-        const int idx = m * 32 + lane;
-        const bool valid = idx < n;
-        const uint32_t v = v_next;  // past the end acts as a terminator
-        v_next = idx + 32 < n ? ldf(f + idx + 32) : 1u;
-        const uint32_t nzm = __ballot_sync(kFull, v != 0);
-        const uint32_t below = nzm & ((1u << lane) - 1u);
-        const int start = below ? m * 32 + (31 - __clz(below)) + 1 : run_start;
-        uint32_t t1 = 0, t2 = 0;
-        int l1 = 0, l2 = 0;
-        if (valid && v != 0) {
-          if (start < idx) {  // the preceding symbol was zero: close its run
-            t1 = static_cast<uint32_t>(idx - start - 1) * 2;
-            l1 = varint_len(t1);
-          }
-          t2 = v * 2 - 1;
-          l2 = varint_len(t2);
-        } else if (valid && idx == n - 1) {
-          t1 = static_cast<uint32_t>(idx - start) * 2;
-          l1 = varint_len(t1);
+      const int nch = (n + 127) >> 7;
+      uint32_t nx[4];
+      auto load = [&](int m) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int idx = m * 128 + 4 * lane + c;
+          nx[c] = idx < n ? ldf(f + idx) : 0u;
         }
-        const int tlen = l1 + l2;
+      };
+      load(0);
+      for (int m = 0; m < nch; ++m) {
+        const uint32_t v[4] = {nx[0], nx[1], nx[2], nx[3]};
+        if (m + 1 < nch) load(m + 1);
+        const int i0 = m * 128 + 4 * lane;
+        int last_nz = -1;  // this lane's last nonzero symbol
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if (v[c] != 0) last_nz = i0 + c;  // symbols past the end load as zero
+        const uint32_t lanes_nz = __ballot_sync(kFull, last_nz >= 0);
+        const uint32_t below = lanes_nz & ((1u << lane) - 1u);
+        const int prev_nz = __shfl_sync(kFull, last_nz, below ? 31 - __clz(below) : 0);
+        const int start = below ? prev_nz + 1 : run_start;
+        // walk the lane's symbols: emit(t) is called for every token in order
+        auto walk = [&](auto emit) {
+          int st = start;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const int idx = i0 + c;
+            if (idx >= n) break;
+            if (v[c] != 0) {
+              if (st < idx) emit(static_cast<uint32_t>(idx - st - 1) * 2);
+              emit(v[c] * 2 - 1);
+              st = idx + 1;
+            } else if (idx == n - 1) {
+              emit(static_cast<uint32_t>(idx - st) * 2);
+            }
+          }
+        };
+        int tlen = 0;
+        walk([&](uint32_t t) { tlen += varint_len(t); });
         int inc = tlen;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -1513,20 +1548,16 @@ enc_emit_kernel(const FrameState* __restrict__ state, EmitRegion ra, EmitRegion 
           if (lane >= o) inc += x;
         }
         int pos = cursor + inc - tlen;
-        for (int b = 0; b < l1; ++b) {
-          uint32_t byte = t1 & 0x7f;
-          t1 >>= 7;
-          if (t1) byte |= 0x80;
-          put_byte(buf, pos++, byte);
-        }
-        for (int b = 0; b < l2; ++b) {
-          uint32_t byte = t2 & 0x7f;
-          t2 >>= 7;
-          if (t2) byte |= 0x80;
-          put_byte(buf, pos++, byte);
-        }
+        walk([&](uint32_t t) {
+          do {
+            uint32_t byte = t & 0x7f;
+            t >>= 7;
+            if (t) byte |= 0x80;
+            put_byte(buf, pos++, byte);
+          } while (t);
+        });
         cursor += __shfl_sync(kFull, inc, 31);
-        run_start = nzm ? m * 32 + (31 - __clz(nzm)) + 1 : run_start;
+        if (lanes_nz) run_start = __shfl_sync(kFull, last_nz, 31 - __clz(lanes_nz)) + 1;
       }
     } else if (mode >= kModeRiceBase && mode <= kModeRiceBase + kMaxRice) {
       // Rice lane c holds symbols c, c+4, ... (encode.cu:556-597; a shard of
@@ -1639,7 +1670,7 @@ enc_emit_kernel(const FrameState* __restrict__ state, EmitRegion ra, EmitRegion 
     // copy out: record bytes [0, rec_len) -> out + offset; byte stores up to
     // the first 16-byte boundary of the destination, then one 16-byte store
     // per lane (five record words funnel-shifted), then the ragged tail
-    uint8_t* dst = outs[si.frame] + si.offset;
+    uint8_t* dst = dst_base + si.offset;
     const uint8_t* bytes = reinterpret_cast<const uint8_t*>(buf);
     const int head = static_cast<int>((16 - (reinterpret_cast<uintptr_t>(dst) & 15)) & 15);
     const int hb = min(head, rec_len);

@@ -95,6 +95,7 @@ struct EmitRegion {
   const ShardInfo* shards;
   const void* folded;
   const uint8_t* rans_scratch;
+  int64_t count;  // shards 0 .. count-1 have records in this region
 };
 void enc_emit_launch(bool fold16, int grid, size_t smem, cudaStream_t stream, const FrameState* state,
                      EmitRegion a, EmitRegion b, int64_t total_shards, uint8_t* const* outs);
