@@ -1561,11 +1561,13 @@ enc_emit_kernel(const FrameState* __restrict__ state, EmitRegion ra, EmitRegion 
       }
     } else if (mode >= kModeRiceBase && mode <= kModeRiceBase + kMaxRice) {
       // Rice lane c holds symbols c, c+4, ... (encode.cu:556-597; a shard of
-      // n < 4 symbols has n lanes of one symbol).  The warp takes 128 symbols
-      // at a time, lane j holding symbols 4j..4j+3: component c of every lane
-      // is then 32 consecutive codes of Rice lane c, placed by one warp scan
-      // of their lengths.  The next 128 symbols are loaded while these are
-      // placed.
+      // n < 4 symbols has n lanes of one symbol).  The warp takes 256 symbols
+      // at a time as two halves of 128, lane j holding symbols 4j..4j+3 of
+      // each: component c of a half is then 32 consecutive codes of Rice
+      // lane c, placed by one warp scan of their lengths; the eight scans of
+      // a step are independent and run interleaved, and the second half's
+      // codes follow the first's.  The next 256 symbols are loaded while
+      // these are placed.
       const int lane_count = min(4, n);
       put_words(buf, 3, lane < lane_count - 1 ? static_cast<uint32_t>(si.comp_lane[lane]) : 0u, lane_count - 1,
                 lane);
@@ -1579,33 +1581,49 @@ enc_emit_kernel(const FrameState* __restrict__ state, EmitRegion ra, EmitRegion 
         }
       }
       const uint32_t rmask = k == 0 ? 0u : (1u << k) - 1u;
-      const int nch = (n + 127) >> 7;
-      uint32_t nx[4];
+      const int nch = (n + 255) >> 8;
+      uint32_t nx[8];  // element 4h + c: symbol 128h + 4 lane + c of the step
       auto load = [&](int m) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int idx = m * 128 + 4 * lane + c;
-          nx[c] = idx < n ? ldf(f + idx) : 0u;
+        for (int i = 0; i < 8; ++i) {
+          const int idx = m * 256 + 128 * (i >> 2) + 4 * lane + (i & 3);
+          nx[i] = idx < n ? ldf(f + idx) : 0u;
         }
       };
       load(0);
       for (int m = 0; m < nch; ++m) {
-        const uint32_t x[4] = {nx[0], nx[1], nx[2], nx[3]};
+        uint32_t x[8], len[8], inc[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = nx[i];
         if (m + 1 < nch) load(m + 1);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const bool valid = m * 128 + 4 * lane + c < n;
-          const uint32_t v = x[c];
-          const uint32_t q = v >> k;
-          const uint32_t len = valid ? q + 1 + k : 0u;
-          uint32_t inc = len;
+        for (int i = 0; i < 8; ++i) {
+          const bool valid = m * 256 + 128 * (i >> 2) + 4 * lane + (i & 3) < n;
+          len[i] = valid ? (x[i] >> k) + 1 + k : 0u;
+          inc[i] = len[i];
+        }
 #pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t2 = __shfl_up_sync(kFull, inc, o);
-            if (lane >= o) inc += t2;
+        for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const uint32_t t2 = __shfl_up_sync(kFull, inc[i], o);
+            if (lane >= o) inc[i] += t2;
           }
-          if (valid) or_bits(buf, bb[c] + inc - len + q, 1u | ((v & rmask) << 1), k + 1);
-          bb[c] += __shfl_sync(kFull, inc, 31);
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const uint32_t tot0 = __shfl_sync(kFull, inc[c], 31);
+          const uint32_t tot1 = __shfl_sync(kFull, inc[4 + c], 31);
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int i = 4 * h + c;
+            if (len[i]) {
+              const uint32_t v = x[i];
+              const int64_t at = bb[c] + (h ? tot0 : 0u) + inc[i] - len[i] + (v >> k);
+              or_bits(buf, at, 1u | ((v & rmask) << 1), k + 1);
+            }
+          }
+          bb[c] += tot0 + tot1;
         }
       }
     } else if (mode == kModeBlockPack) {
