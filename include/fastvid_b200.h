@@ -275,12 +275,13 @@ int fvb_bucket_decode_enqueue(const fvb_bucket* bucket, int wavefront, void* wor
  * runs on the caller's stream).  Every GPU that loads the library holds the
  * array until the process exits.  The first call on a device does the
  * set-up: it looks up the array's device address (cudaGetSymbolAddress) and
- * sets the kernels' shared-memory limits; make that first call before any
- * stream capture.  The stream and the planes must be device (or managed)
- * memory.  All calls share the one array, which keeps the last call's
- * contents (every decode rewrites what it reads): calls whose work overlaps
- * on the GPU (other threads, other streams) race and must be serialised by
- * the caller; the call itself waits for its result before returning. */
+ * sets the kernels' shared-memory limits.  The call is synchronous -- it
+ * waits for its result before returning -- so it cannot be captured into a
+ * CUDA graph: never call it on a stream that is being captured.  The stream
+ * and the planes must be device (or managed) memory.  All calls share the
+ * one array, which keeps the last call's contents (every decode rewrites
+ * what it reads): calls whose work overlaps on the GPU (other threads, other
+ * streams) race and must be serialised by the caller. */
 int64_t fvb_decode_noalloc_capacity(void);
 int fvb_decode_noalloc(const fvb_frame* frame, const uint8_t* stream, int64_t stream_len, uint16_t* const* planes,
                        const int64_t* pitches, int wavefront, void* cuda_stream);
