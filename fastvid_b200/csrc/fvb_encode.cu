@@ -1449,6 +1449,65 @@ __device__ __forceinline__ void put_bytes(uint32_t* buf, int pos, const uint8_t*
   }
 }
 
+// put_bytes over the five pieces of an order-0 record held in memory (the
+// serialised table, then the four lanes), with the loads of every piece's
+// next 64 words issued before any is merged: the record then costs as many
+// load latencies as its longest piece has rounds, not their sum.
+__device__ __forceinline__ void put_pieces(uint32_t* buf, const uint8_t* const (&src)[5], const int (&pos)[5],
+                                           const int (&len)[5], int lane) {
+  int span = 0;  // destination words of the longest piece
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+    if (len[i] > 0) span = max(span, ((pos[i] + len[i] - 1) >> 2) - (pos[i] >> 2) + 1);
+  for (int off = 0; off < span; off += 64) {
+    uint32_t la[5], lb[5], ta[5], tb[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const uintptr_t sa = reinterpret_cast<uintptr_t>(src[i]);
+      const uint32_t* __restrict__ sw = reinterpret_cast<const uint32_t*>(sa & ~static_cast<uintptr_t>(3));
+      const int h = static_cast<int>(sa & 3);
+      const int last_w = len[i] > 0 ? (h + len[i] - 1) >> 2 : -1;
+      const int qb = h - pos[i];
+      const int d1 = len[i] > 0 ? min((pos[i] + len[i] - 1) >> 2, kEmitWords - 1) : -1;
+      const int dd = (pos[i] >> 2) + off;
+      auto word = [&](int wi) { return (wi >= 0 && wi <= last_w) ? __ldg(sw + wi) : 0u; };
+      const int wa = (qb + 4 * (dd + lane)) >> 2, wb = (qb + 4 * (dd + 32 + lane)) >> 2;  // floor
+      la[i] = dd <= d1 ? word(wa) : 0u;
+      lb[i] = dd + 32 <= d1 ? word(wb) : 0u;
+      ta[i] = (lane == 31 && dd <= d1) ? word(wa + 1) : 0u;
+      tb[i] = (lane == 31 && dd + 32 <= d1) ? word(wb + 1) : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const int h = static_cast<int>(reinterpret_cast<uintptr_t>(src[i]) & 3);
+      const int qb = h - pos[i];
+      const int sh = 8 * (qb & 3);
+      const int d1 = len[i] > 0 ? min((pos[i] + len[i] - 1) >> 2, kEmitWords - 1) : -1;
+      const int dd = (pos[i] >> 2) + off;
+      uint32_t ha = __shfl_down_sync(kFull, la[i], 1);
+      uint32_t hb = __shfl_down_sync(kFull, lb[i], 1);
+      if (lane == 31) {
+        ha = ta[i];
+        hb = tb[i];
+      }
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int d = dd + 32 * r + lane;
+        if (d > d1) continue;
+        const uint32_t v = __funnelshift_r(r ? lb[i] : la[i], r ? hb : ha, sh);
+        const int s0 = 4 * d - pos[i];  // piece offset of record byte 4d (>= -3)
+        if (s0 >= 0 && s0 + 3 < len[i]) {
+          buf[d] = v;
+        } else {
+          const int k0 = max(0, -s0), k1 = min(3, len[i] - 1 - s0);
+          const uint32_t mask = (0xffffffffu >> (8 * (3 - k1))) & (0xffffffffu << (8 * k0));
+          atomicOr(&buf[d], v & mask);
+        }
+      }
+    }
+  }
+}
+
 // Record bytes [pos, pos + 4n) <- the 32-bit little-endian values v held by
 // lanes 0..n-1 (lane i's value at pos + 4i), merged with shared atomics.
 __device__ __forceinline__ void put_words(uint32_t* buf, int pos, uint32_t v, int n, int lane) {
@@ -1670,19 +1729,25 @@ enc_emit_kernel(const FrameState* __restrict__ state, EmitRegion ra, EmitRegion 
       const uint8_t* base = rans_scratch + s * static_cast<int64_t>(kRansScratchBytes);
       const uint8_t* ser = base + kRansTableWords * 4;
       const int tb = body - 28 - si.comp_lane[0] - si.comp_lane[1] - si.comp_lane[2] - si.comp_lane[3];
-      put_bytes(buf, 3, ser, tb, lane);
-      int pos = 3 + tb;
       // three lane lengths, then four final states: seven words from lanes 0..6
       const uint32_t lw = lane < 3 ? static_cast<uint32_t>(si.comp_lane[lane])
                                    : (lane < 7 ? si.rans_state[lane - 3] : 0u);
-      put_words(buf, pos, lw, 7, lane);
-      pos += 28;
+      put_words(buf, 3 + tb, lw, 7, lane);
+      // the table at byte 3, the lanes after the 28 bytes of lengths and states
+      const uint8_t* src[5];
+      int pos[5], len[5];
+      src[0] = ser;
+      pos[0] = 3;
+      len[0] = tb;
+      int p = 31 + tb;
+#pragma unroll
       for (int l = 0; l < 4; ++l) {
-        const int len = si.comp_lane[l];
-        const uint8_t* lane_end = base + kRansTableWords * 4 + kRansSerialBytes + (l + 1) * kRansLaneBytes;
-        put_bytes(buf, pos, lane_end - len, len, lane);
-        pos += len;
+        len[l + 1] = si.comp_lane[l];
+        src[l + 1] = base + kRansTableWords * 4 + kRansSerialBytes + (l + 1) * kRansLaneBytes - len[l + 1];
+        pos[l + 1] = p;
+        p += len[l + 1];
       }
+      put_pieces(buf, src, pos, len, lane);
     }
     __syncwarp();
     // copy out: record bytes [0, rec_len) -> out + offset; byte stores up to
