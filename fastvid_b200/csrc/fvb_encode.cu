@@ -1066,7 +1066,10 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
   const int first = n - 1 - ((n - 1 - lane) & 3);
   const int steps = first >= 0 ? first / 4 + 1 : 0;  // symbols first, first-4, ..., >= 0
   // one encoding step (encode.cu:401-418): renormalise -- at most two bytes,
-  // since x < 2^31 and the threshold f * 2^19 >= 2^19 -- then the state map
+  // since x < 2^31 and the threshold f * 2^19 >= 2^19 -- then the state map.
+  // Pending bytes are written out a word at a time by flush(): after a pair
+  // of steps (at most 3 + 4 = 7 pending, one word written leaves at most 3),
+  // or after every step of an odd tail.
   auto step = [&](uint2 e) {
     const uint32_t cmpl = (e.y >> 13) & 0xfffu;
     const uint32_t thr = (4096u - cmpl) << 19;  // ((L >> 12) << 8) * f
@@ -1077,13 +1080,15 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
     ahi = __funnelshift_l(alo, ahi, sh);
     alo = (alo << sh) | (nb ? bytes : 0u);
     nacc += nb;
-    if (nacc >= 4) {
-      nacc -= 4;
-      out_end[-(++nwords)] = __funnelshift_r(alo, ahi, 8 * nacc);  // (ahi:alo) >> 8 nacc, nacc 0 or 1
-    }
     x >>= sh;
     const uint32_t q = __umulhi(x, e.x) >> (e.y >> 25);
     x += (e.y & 0x1fffu) + q * cmpl;
+  };
+  auto flush = [&]() {
+    if (nacc >= 4) {
+      nacc -= 4;
+      out_end[-(++nwords)] = __funnelshift_r(alo, ahi, 8 * nacc);  // (ahi:alo) >> 8 nacc, nacc 0..3
+    }
   };
   int c = 0;
   if (PIPE == 0) {
@@ -1097,14 +1102,18 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
 #pragma unroll
       for (int j = 0; j < kAhead; ++j) e[j] = tab[v[j]];
 #pragma unroll
-      for (int j = 0; j < kAhead; ++j) step(e[j]);
+      for (int j = 0; j < kAhead; j += 2) {
+        step(e[j]);
+        step(e[j + 1]);
+        flush();
+      }
     }
   } else {
     // Software pipeline over blocks of PIPE steps: while block b runs, the
     // table entries of block b+1 (whose symbols arrived a block earlier) and
     // the symbols of block b+2 are in flight, so neither the symbol load nor
     // the dependent table load sits on the state chain.
-    constexpr int kB = PIPE > 0 ? PIPE : 1;
+    constexpr int kB = PIPE > 0 ? PIPE : 2;  // even: steps go in pairs
     const int nblk = steps / kB;
     uint32_t vn[kB];      // symbols of block b+2
     uint2 en[kB], ec[kB];  // table entries of blocks b+1 and b
@@ -1136,11 +1145,18 @@ enc_rans_kernel(const FrameState* __restrict__ state, const BatchDims* __restric
       }
       if (b + 3 < nblk) load_v(b + 3, vn);
 #pragma unroll
-      for (int j = 0; j < kB; ++j) step(cur[j]);
+      for (int j = 0; j < kB; j += 2) {
+        step(cur[j]);
+        step(cur[j + 1]);
+        flush();
+      }
     }
     c = nblk * kB;
   }
-  for (; c < steps; ++c) step(tab[ldf(f + first - 4 * c)]);
+  for (; c < steps; ++c) {
+    step(tab[ldf(f + first - 4 * c)]);
+    flush();
+  }
   if (nacc) out_end[-(nwords + 1)] = alo << (8 * (4 - nacc));  // low bytes unused
   si.rans_lane[lane] = 4 * nwords + nacc;
   si.rans_state[lane] = x;
