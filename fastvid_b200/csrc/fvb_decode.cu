@@ -126,11 +126,20 @@ __global__ void dec_parse_kernel(const FrameDesc* __restrict__ frames, FrameStat
       set_status(&st.status, 11);
       continue;
     }
-    // bin the tile's shards by entropy mode for dec_shards
+    // bin the tile's shards by entropy mode for dec_shards; the lanes that
+    // bin into the same list together take their slots with one atomic
+    // (every shard of a batch lands on one of four counters)
+    const int lane = static_cast<int>(threadIdx.x & 31);
     for (int j = 0; j < g.shard_count; ++j) {
       const int64_t s = f.shard_base + g.first_shard + j;
       const int list = list_of_mode(shards[s].mode);
-      const int pos = atomicAdd(&lists->count[list], 1);
+      const unsigned active = __activemask();
+      const unsigned peers = __match_any_sync(active, list);
+      const int leader = __ffs(peers) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(&lists->count[list], __popc(peers));
+      base = __shfl_sync(peers, base, leader);
+      const int pos = base + __popc(peers & ((1u << lane) - 1u));
       list_items[static_cast<int64_t>(list) * total_shards + pos] = static_cast<int32_t>(s);
     }
   }

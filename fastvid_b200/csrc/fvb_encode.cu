@@ -1550,8 +1550,9 @@ enc_emit_kernel(const FrameState* __restrict__ state, EmitRegion ra, EmitRegion 
     const ShardInfo& si = (from_b ? rb.shards : ra.shards)[s];
     {  // the next shard's record into L1 while this one is assembled
       const int64_t sn = s + warps_total;
-      if (lane < 2 && sn < total_shards)
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(reinterpret_cast<const char*>(ra.shards + sn) + 64 * lane));
+      if (lane < 2 && sn < total_shards)  // its first and last byte: the record spans at most two lines
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(reinterpret_cast<const char*>(ra.shards + sn) +
+                                                      (lane ? sizeof(ShardInfo) - 1 : 0)));
     }
     const FoldT* __restrict__ folded = static_cast<const FoldT*>(from_b ? rb.folded : ra.folded);
     const uint8_t* __restrict__ rans_scratch = from_b ? rb.rans_scratch : ra.rans_scratch;
